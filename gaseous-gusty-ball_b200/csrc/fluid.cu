@@ -1,0 +1,610 @@
+// fluid.cu — the fluid.h entry points of libggb_cuda.so: discrete operators,
+// the multigrid hierarchy, the Poisson solve launch, velocity from the stream
+// function and the BFECC semi-Lagrangian vorticity step.
+//
+// Upstream: src/fluid.c.  Public arrays of Fluid are managed memory updated in
+// place by the kernels below; every entry point synchronises before returning.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "ggb_internal.h"
+#include "ggb_solver.h"
+
+namespace ggb {
+
+int pcg_grid_size();
+int pcg_block_size();
+void pcg_launch(const SolveParams &prm, cudaStream_t s);
+
+constexpr int kB = 256;
+
+// ------------------------------------------------------------ operators
+
+// upstream src/fluid.c:214-230
+__global__ void k_divergence(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *elen,
+                             const float *area, const float *vel, float *div) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        D3 p = load3(pos + 3 * i), ui = load3(vel + 3 * i);
+        double s = 0;
+        for (int k = 0; k < nnb[i]; k++) {
+            int j = nbr[kMaxNb * i + k];
+            D3 nrm = normalize(sub(load3(pos + 3 * j), p));
+            D3 um = add(ui, load3(vel + 3 * j));
+            s += elen[kMaxNb * i + k] * 0.5 * dot(um, nrm);
+        }
+        div[i] = (float)(s / area[i]);
+    }
+}
+
+// upstream src/fluid.c:233-250
+__global__ void k_curl(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *elen,
+                       const float *area, const float *vel, float *omega) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        D3 p = load3(pos + 3 * i);
+        D3 wi = cross(load3(vel + 3 * i), p);
+        double s = 0;
+        for (int k = 0; k < nnb[i]; k++) {
+            int j = nbr[kMaxNb * i + k];
+            D3 pj = load3(pos + 3 * j);
+            D3 wj = cross(load3(vel + 3 * j), pj);
+            D3 nrm = normalize(sub(pj, p));
+            s += elen[kMaxNb * i + k] * 0.5 * dot(add(wi, wj), nrm);
+        }
+        omega[i] = (float)(s / area[i]);
+    }
+}
+
+// y = sum_j w (x_j - x_i) / A_i on the face-tiled layout; upstream src/fluid.c:252-262
+__global__ void k_laplacian(StencilDev S, const float *area, const float *x, float *y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += gridDim.x * blockDim.x) {
+        auto X = [&](int k) -> double { return (double)x[k]; };
+        double kx = apply_k(S, i, (double)x[i], X);
+        y[i] = (float)(-kx / area[i]);
+    }
+}
+
+// Per-block FP64 partials of sum A f, then a one-block fixed-order total.
+__global__ void k_wsum_partial(int n, const float *area, const float *f, double *part) {
+    __shared__ double s_red[kB / 32 + 2];
+    double s = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        s += (double)area[i] * f[i];
+    double t = block_sum<kB>(s, s_red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_remove_mean(int n, const double *part, int nparts, double total_area, float *f) {
+    __shared__ double s_red[kB / 32 + 2];
+    double s = sum_partials<kB>(part, nparts, s_red);
+    float m = (float)(s / total_area);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f[i] -= m;
+}
+
+// u = p x sum_k gc_k (psi_j - psi_i); upstream src/fluid.c:361-376
+__global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *gc,
+                           const float *psi, float *vel) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        D3 p = load3(pos + 3 * i), g = d3(0, 0, 0);
+        double pi = psi[i];
+        int m = nnb[i];
+        for (int k = 0; k < m; k++) {
+            int j = __ldg(nbr + kMaxNb * i + k);
+            g = add(g, scale(load3(gc + 3 * (kMaxNb * i + k)), psi[j] - pi));
+        }
+        store3(vel + 3 * i, cross(p, g));
+    }
+}
+
+// max |u|^2 (formed in FP32 like upstream src/fluid.c:480-491) as float bits.
+__global__ void k_max_speed2(int n, const float *vel, unsigned int *out) {
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float *v = vel + 3 * i;
+        float s = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        m = fmaxf(m, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// ------------------------------------------------------------ advection
+
+// Midpoint backtraces (backward and, for BFECC, forward) and q0 = omega + 2 Omega y.
+// upstream src/fluid.c:397-414, 435-437
+__global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt,
+                             double two_omega, int forward, float *dep_b, float *dep_f, float *q0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        D3 p = load3(pos + 3 * i), u = load3(vel + 3 * i);
+        D3 pm = sphere_move(p, u, -0.5 * dt);
+        D3 um = tangent(sample_vec(g, vel, pm), p);
+        store3(dep_b + 3 * i, sphere_move(p, um, -dt));
+        if (forward) {
+            pm = sphere_move(p, u, 0.5 * dt);
+            um = tangent(sample_vec(g, vel, pm), p);
+            store3(dep_f + 3 * i, sphere_move(p, um, dt));
+        }
+        q0[i] = (float)(omega[i] + two_omega * pos[3 * i + 1]);
+    }
+}
+
+// dst = src sampled at dep; with `correct`, dst = q0 + 0.5 (q0 - dst)
+// (the BFECC corrected source, upstream src/fluid.c:445-448).
+__global__ void k_resample(GridDev g, const float *src, const float *dep, const float *q0, int correct, float *dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        float v = (float)sample_scalar(g, src, load3(dep + 3 * i));
+        if (correct) {
+            float q = q0[i];
+            v = q + 0.5f * (q - v);
+        }
+        dst[i] = v;
+    }
+}
+
+// Limited resample of the corrected source at dep_b (clamped to the range of
+// q0 over the same taps), then back to relative vorticity and relaxation
+// toward the band state.  upstream src/fluid.c:449-474
+__global__ void k_limit_relax(GridDev g, const float *pos, const float *dep_b, const float *q0, const float *q2,
+                              int bfecc, double two_omega, double relax, const float *omega_band, float *q1,
+                              float *omega) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        float qn;
+        if (bfecc) {
+            int idx[4];
+            double wt[4];
+            taps(g, load3(dep_b + 3 * i), idx, wt);
+            double v = 0, lo = 1e30, hi = -1e30;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                v += wt[k] * q2[idx[k]];
+                double o = q0[idx[k]];
+                lo = o < lo ? o : lo;
+                hi = o > hi ? o : hi;
+            }
+            v = v < lo ? lo : v;
+            v = v > hi ? hi : v;
+            qn = (float)v;
+            q1[i] = qn;
+        } else {
+            qn = q1[i];
+        }
+        double w = qn - two_omega * pos[3 * i + 1];
+        w += relax * (omega_band[i] - w);
+        omega[i] = (float)w;
+    }
+}
+
+// ------------------------------------------------------------ multigrid setup
+
+// Fine cell i -> bilinear taps on the coarse grid at its (FP32-stored) centre.
+// upstream src/fluid.c:70-79
+__global__ void k_ptaps(int nf, const float *fine_pos, GridDev coarse, int *ptap, float *pw, int *rcount) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x) {
+        int idx[4];
+        double wt[4];
+        taps(coarse, load3(fine_pos + 3 * i), idx, wt);
+        for (int k = 0; k < 4; k++) {
+            ptap[4 * i + k] = idx[k];
+            pw[4 * i + k] = (float)wt[k];
+            atomicAdd(rcount + idx[k] + 1, 1);
+        }
+    }
+}
+
+// Exclusive prefix sum in place over a[0..n] (one block; setup only).
+__global__ void k_scan_inplace(int n, int *a) {
+    __shared__ int s_tot[1024];
+    const int T = blockDim.x, t = threadIdx.x;
+    int chunk = (n + T - 1) / T, lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    int s = 0;
+    for (int k = lo; k < hi; k++) s += a[k];
+    s_tot[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int acc = 0;
+        for (int k = 0; k < T; k++) {
+            int v = s_tot[k];
+            s_tot[k] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    int acc = s_tot[t];
+    for (int k = lo; k < hi; k++) {
+        int v = a[k];
+        a[k] = acc;
+        acc += v;
+    }
+}
+
+__global__ void k_rfill(int nf, const int *ptap, const int *rstart, int *cursor, int *rkey) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x)
+        for (int k = 0; k < 4; k++) {
+            int c = ptap[4 * i + k];
+            int slot = atomicAdd(cursor + c, 1);
+            rkey[rstart[c] + slot] = 4 * i + k;
+        }
+}
+
+// Sort each row by (fine cell, tap) — the fill order of upstream src/fluid.c:88-95.
+__global__ void k_rsort(int nc, const int *rstart, int *rkey, const float *pw, int *ridx, float *rw) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        int a = rstart[c], b = rstart[c + 1];
+        for (int u = a + 1; u < b; u++) {
+            int key = rkey[u], v = u - 1;
+            while (v >= a && rkey[v] > key) {
+                rkey[v + 1] = rkey[v];
+                v--;
+            }
+            rkey[v + 1] = key;
+        }
+        for (int u = a; u < b; u++) {
+            ridx[u] = rkey[u] >> 2;
+            rw[u] = pw[rkey[u]];
+        }
+    }
+}
+
+// ------------------------------------------------------------ private state
+
+struct FluidPriv {
+    MGLevel lev[kMaxLev];  // public view; first member (Fluid::lev points here)
+    GridTables *grid0 = nullptr;
+    GridTables coarse[kMaxLev];
+    int nlev = 0;
+    int *ptap[kMaxLev] = {}, *rstart[kMaxLev] = {}, *ridx[kMaxLev] = {};
+    float *pw[kMaxLev] = {}, *rw[kMaxLev] = {};
+    float *lx[kMaxLev] = {}, *lxo[kMaxLev] = {}, *lb[kMaxLev] = {}, *lr[kMaxLev] = {};
+    float *r2 = nullptr, *p2 = nullptr;
+    double *part = nullptr;
+    double *wpart = nullptr;
+    GridBarrier *bar = nullptr;
+    SolveResult *res = nullptr;
+    SolveResult *res_host = nullptr;
+    unsigned int *vmax_bits = nullptr;
+    unsigned int *vmax_host = nullptr;
+};
+
+static FluidPriv *priv_of(const Fluid *F) {
+    if (!F->lev) fail_msg("Fluid %p was not initialised by this library's fluid_init", (const void *)F);
+    return reinterpret_cast<FluidPriv *>(F->lev);
+}
+
+static StencilDev stencil_of(const GridTables *t) {
+    StencilDev s;
+    s.N = t->N;
+    s.n = t->n;
+    s.nring = t->nring;
+    s.wslot = t->wslot;
+    s.ring_nb = t->ring_nb;
+    s.ring_w = t->ring_w;
+    return s;
+}
+
+static unsigned blocks_for(int n) { return std::max(1u, std::min<unsigned>(grid_for(n, kB), 148u * 16u)); }
+
+static void build_levels(Fluid *F, FluidPriv *Pv) {
+    cudaStream_t s = stream();
+    int N = F->cs->N, nlev = 1;
+    while ((N >> nlev) >= 4 && ((N >> (nlev - 1)) % 2) == 0) nlev++;
+    if (nlev > kMaxLev) nlev = kMaxLev;
+    Pv->nlev = nlev;
+    for (int l = 1; l < nlev; l++) {
+        GridTables *C = &Pv->coarse[l];
+        if (grid_build(C, N >> l, false) != 0) fail_msg("multigrid level %d (N=%d) failed", l, N >> l);
+        const GridTables *Fg = l == 1 ? Pv->grid0 : &Pv->coarse[l - 1];
+        int nf = Fg->n, nc = C->n;
+        int L = l - 1;
+        Pv->ptap[L] = (int *)dev_alloc(sizeof(int) * 4 * nf);
+        Pv->pw[L] = (float *)dev_alloc(sizeof(float) * 4 * nf);
+        Pv->rstart[L] = (int *)dev_alloc(sizeof(int) * (nc + 1));
+        Pv->ridx[L] = (int *)dev_alloc(sizeof(int) * 4 * nf);
+        Pv->rw[L] = (float *)dev_alloc(sizeof(float) * 4 * nf);
+        int *cursor = (int *)dev_alloc(sizeof(int) * nc);
+        int *rkey = (int *)dev_alloc(sizeof(int) * 4 * nf);
+        k_ptaps<<<blocks_for(nf), kB, 0, s>>>(nf, Fg->pos, C->dev(), Pv->ptap[L], Pv->pw[L], Pv->rstart[L]);
+        GGB_LAUNCHED();
+        k_scan_inplace<<<1, 1024, 0, s>>>(nc + 1, Pv->rstart[L]);
+        GGB_LAUNCHED();
+        k_rfill<<<blocks_for(nf), kB, 0, s>>>(nf, Pv->ptap[L], Pv->rstart[L], cursor, rkey);
+        GGB_LAUNCHED();
+        k_rsort<<<blocks_for(nc), kB, 0, s>>>(nc, Pv->rstart[L], rkey, Pv->pw[L], Pv->ridx[L], Pv->rw[L]);
+        GGB_LAUNCHED();
+        GGB_CHECK(cudaStreamSynchronize(s));
+        dev_free(cursor);
+        dev_free(rkey);
+    }
+    for (int l = 0; l < nlev; l++) {
+        int n = l == 0 ? Pv->grid0->n : Pv->coarse[l].n;
+        Pv->lx[l] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lxo[l] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lb[l] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lr[l] = (float *)dev_alloc(sizeof(float) * n);
+    }
+    F->nlev = nlev;
+    for (int l = 0; l < nlev; l++) {
+        MGLevel *M = &Pv->lev[l];
+        memset(M, 0, sizeof(*M));
+        const GridTables *t = l == 0 ? Pv->grid0 : &Pv->coarse[l];
+        M->cs.N = t->N;
+        M->cs.ncells = t->n;
+        M->cs.h = t->h;
+        M->cs.total_area = t->total_area;
+    }
+}
+
+constexpr int kBlockLevelMax = 6144;  // levels up to N=32 run inside one block
+
+static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
+    SolveParams P;
+    memset(&P, 0, sizeof(P));
+    const bool mg = F->prm.multigrid != 0;
+    P.nlev = mg ? Pv->nlev : 0;
+    P.coarse_sweeps = 60;
+    P.remove_mean = remove_mean;
+    P.maxit = maxit;
+    P.tol = F->prm.cg_tol;
+    P.total_area = Pv->grid0->total_area;
+    for (int l = 0; l < (mg ? Pv->nlev : 1); l++) {
+        const GridTables *t = l == 0 ? Pv->grid0 : &Pv->coarse[l];
+        LevelDev &L = P.L[l];
+        L.S = stencil_of(t);
+        L.dinv = t->dinv;
+        L.x = Pv->lx[l] ? Pv->lx[l] : nullptr;
+        L.xo = Pv->lxo[l];
+        L.b = Pv->lb[l];
+        L.r = Pv->lr[l];
+        if (l + 1 < Pv->nlev) {
+            L.ptap = Pv->ptap[l];
+            L.pw = Pv->pw[l];
+            L.rstart = Pv->rstart[l];
+            L.ridx = Pv->ridx[l];
+            L.rw = Pv->rw[l];
+        }
+    }
+    if (mg && Pv->nlev >= 2) {
+        int G = 0;
+        while (G < Pv->nlev - 1 && P.L[G].S.n > kBlockLevelMax) G++;
+        if (G < 1) G = 1;
+        P.nlev_grid = G;
+        P.coarse_on_grid = (G == Pv->nlev - 1 && P.L[Pv->nlev - 1].S.n > kBlockLevelMax) ? 1 : 0;
+    } else if (mg) {
+        P.nlev_grid = 0;
+        P.coarse_on_grid = P.L[0].S.n > kBlockLevelMax ? 1 : 0;
+    }
+    P.area = F->cs->area;
+    P.omega = F->omega;
+    P.psi = F->psi;
+    P.r = F->r;
+    P.r2 = Pv->r2;
+    P.p = F->p;
+    P.p2 = Pv->p2;
+    P.Ap = F->Ap;
+    P.z = F->z;
+    P.part = Pv->part;
+    P.bar = Pv->bar;
+    P.res = Pv->res;
+    return P;
+}
+
+// Launch the solve and read back its result into F (sync).
+static int run_solve(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
+    SolveParams P = solve_params(F, Pv, remove_mean, maxit);
+    cudaStream_t s = stream();
+    pcg_launch(P, s);
+    GGB_CHECK(cudaMemcpyAsync(Pv->res_host, Pv->res, sizeof(SolveResult), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaStreamSynchronize(s));
+    const SolveResult &R = *Pv->res_host;
+    if (R.status != 0) fail_msg("Poisson solve aborted: a grid barrier timed out");
+    F->cg_iters = R.iters;
+    F->cg_relres = R.relres;
+    return R.iters;
+}
+
+}  // namespace ggb
+
+using namespace ggb;
+
+// ------------------------------------------------------------ public API
+
+GGB_EXPORT void fluid_divergence(const CubeSphere *cs, const float *vel, float *div) {
+    GridTables *t = grid_lookup(cs);
+    Staged in, out;
+    stage_in(in, vel, sizeof(float) * 3 * t->n);
+    stage_out(out, div, sizeof(float) * t->n);
+    k_divergence<<<blocks_for(t->n), kB, 0, stream()>>>(t->n, t->pos, t->nnb, t->nbr, t->elen, t->area,
+                                                        (const float *)in.dev, (float *)out.dev);
+    GGB_LAUNCHED();
+    stage_finish(out);
+}
+
+GGB_EXPORT void fluid_curl(const CubeSphere *cs, const float *vel, float *omega) {
+    GridTables *t = grid_lookup(cs);
+    Staged in, out;
+    stage_in(in, vel, sizeof(float) * 3 * t->n);
+    stage_out(out, omega, sizeof(float) * t->n);
+    k_curl<<<blocks_for(t->n), kB, 0, stream()>>>(t->n, t->pos, t->nnb, t->nbr, t->elen, t->area,
+                                                  (const float *)in.dev, (float *)out.dev);
+    GGB_LAUNCHED();
+    stage_finish(out);
+}
+
+GGB_EXPORT void fluid_laplacian(const CubeSphere *cs, const float *x, float *y) {
+    GridTables *t = grid_lookup(cs);
+    Staged in, out;
+    stage_in(in, x, sizeof(float) * t->n);
+    stage_out(out, y, sizeof(float) * t->n);
+    k_laplacian<<<blocks_for(t->n), kB, 0, stream()>>>(stencil_of(t), t->area, (const float *)in.dev,
+                                                       (float *)out.dev);
+    GGB_LAUNCHED();
+    stage_finish(out);
+}
+
+GGB_EXPORT void fluid_remove_mean(const CubeSphere *cs, float *f) {
+    GridTables *t = grid_lookup(cs);
+    Staged io;
+    stage_in(io, f, sizeof(float) * t->n);
+    unsigned nb = std::min(blocks_for(t->n), 1024u);
+    double *part = (double *)dev_alloc(sizeof(double) * nb);
+    k_wsum_partial<<<nb, kB, 0, stream()>>>(t->n, t->area, (const float *)io.dev, part);
+    GGB_LAUNCHED();
+    k_remove_mean<<<blocks_for(t->n), kB, 0, stream()>>>(t->n, part, nb, t->total_area, (float *)io.dev);
+    GGB_LAUNCHED();
+    if (io.owned) {
+        io.bytes = sizeof(float) * t->n;
+        stage_finish(io);
+    } else {
+        sync();
+    }
+    dev_free(part);
+}
+
+GGB_EXPORT int fluid_init(Fluid *F, const CubeSphere *cs, const FluidParams *prm) {
+    memset(F, 0, sizeof(*F));
+    FluidPriv *Pv = new FluidPriv();
+    Pv->grid0 = grid_lookup(cs);
+    F->cs = cs;
+    F->prm = *prm;
+    size_t n = cs->ncells;
+    float **fields[] = {&F->omega, &F->omega_band, &F->psi, &F->q0, &F->q1, &F->q2,
+                        &F->r, &F->p, &F->Ap, &F->z, &F->dinv};
+    for (float **f : fields) *f = (float *)managed_alloc(sizeof(float) * n);
+    F->vel = (float *)managed_alloc(sizeof(float) * 3 * n);
+    F->dep_b = (float *)managed_alloc(sizeof(float) * 3 * n);
+    F->dep_f = (float *)managed_alloc(sizeof(float) * 3 * n);
+    Pv->r2 = (float *)dev_alloc(sizeof(float) * n);
+    Pv->p2 = (float *)dev_alloc(sizeof(float) * n);
+    GGB_CHECK(cudaMemcpyAsync(F->dinv, Pv->grid0->dinv, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream()));
+    F->lev = Pv->lev;
+    if (prm->multigrid) {
+        build_levels(F, Pv);
+    } else {
+        Pv->nlev = 0;
+        Pv->lx[0] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lxo[0] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lb[0] = (float *)dev_alloc(sizeof(float) * n);
+        Pv->lr[0] = (float *)dev_alloc(sizeof(float) * n);
+        F->nlev = 0;
+    }
+    Pv->part = (double *)dev_alloc(sizeof(double) * 8 * pcg_grid_size());
+    Pv->wpart = (double *)dev_alloc(sizeof(double) * 1024);
+    Pv->bar = (GridBarrier *)dev_alloc(sizeof(GridBarrier));
+    Pv->res = (SolveResult *)dev_alloc(sizeof(SolveResult));
+    Pv->vmax_bits = (unsigned int *)dev_alloc(sizeof(unsigned int));
+    GGB_CHECK(cudaMallocHost(&Pv->res_host, sizeof(SolveResult)));
+    GGB_CHECK(cudaMallocHost(&Pv->vmax_host, sizeof(unsigned int)));
+    sync();
+    return 0;
+}
+
+GGB_EXPORT void fluid_free(Fluid *F) {
+    if (!F->lev) {
+        memset(F, 0, sizeof(*F));
+        return;
+    }
+    FluidPriv *Pv = priv_of(F);
+    sync();
+    float *fields[] = {F->omega, F->omega_band, F->psi, F->vel, F->q0, F->q1, F->q2,
+                       F->dep_b, F->dep_f, F->r, F->p, F->Ap, F->z, F->dinv};
+    for (float *f : fields) managed_free(f);
+    for (int l = 0; l < kMaxLev; l++) {
+        if (l >= 1 && Pv->coarse[l].n) grid_release(&Pv->coarse[l]);
+        dev_free(Pv->ptap[l]);
+        dev_free(Pv->pw[l]);
+        dev_free(Pv->rstart[l]);
+        dev_free(Pv->ridx[l]);
+        dev_free(Pv->rw[l]);
+        dev_free(Pv->lx[l]);
+        dev_free(Pv->lxo[l]);
+        dev_free(Pv->lb[l]);
+        dev_free(Pv->lr[l]);
+    }
+    dev_free(Pv->r2);
+    dev_free(Pv->p2);
+    dev_free(Pv->part);
+    dev_free(Pv->wpart);
+    dev_free(Pv->bar);
+    dev_free(Pv->res);
+    dev_free(Pv->vmax_bits);
+    cudaFreeHost(Pv->res_host);
+    cudaFreeHost(Pv->vmax_host);
+    delete Pv;
+    memset(F, 0, sizeof(*F));
+}
+
+GGB_EXPORT int fluid_solve_psi(Fluid *F) {
+    FluidPriv *Pv = priv_of(F);
+    return run_solve(F, Pv, 0, F->prm.cg_maxit);
+}
+
+static void launch_velocity(Fluid *F, FluidPriv *Pv) {
+    const GridTables *t = Pv->grid0;
+    k_velocity<<<blocks_for(t->n), kB, 0, stream()>>>(t->n, t->pos, t->nnb, t->nbr, t->gc, F->psi, F->vel);
+    GGB_LAUNCHED();
+}
+
+GGB_EXPORT void fluid_compute_velocity(Fluid *F) {
+    launch_velocity(F, priv_of(F));
+    sync();
+}
+
+// upstream src/fluid.c:378-395
+GGB_EXPORT void fluid_set_state(Fluid *F, const float *vel_initial, const float *vel_band) {
+    FluidPriv *Pv = priv_of(F);
+    const CubeSphere *cs = F->cs;
+    size_t n = cs->ncells;
+    fluid_curl(cs, vel_initial, F->omega);
+    fluid_remove_mean(cs, F->omega);
+    if (vel_band) {
+        fluid_curl(cs, vel_band, F->omega_band);
+        fluid_remove_mean(cs, F->omega_band);
+    } else {
+        GGB_CHECK(cudaMemsetAsync(F->omega_band, 0, sizeof(float) * n, stream()));
+    }
+    GGB_CHECK(cudaMemsetAsync(F->psi, 0, sizeof(float) * n, stream()));
+    int keep = F->prm.cg_maxit;
+    int cold = keep * 20 > 20000 ? keep * 20 : 20000;
+    run_solve(F, Pv, 0, cold);
+    launch_velocity(F, Pv);
+    sync();
+}
+
+// upstream src/fluid.c:424-478
+GGB_EXPORT void fluid_step(Fluid *F, double dt) {
+    FluidPriv *Pv = priv_of(F);
+    const GridTables *t = Pv->grid0;
+    cudaStream_t s = stream();
+    double two_omega = 2.0 * F->prm.rotation;
+    int bfecc = F->prm.bfecc != 0;
+    GridDev g = t->dev();
+    unsigned nb = blocks_for(t->n);
+    k_departures<<<nb, kB, 0, s>>>(g, t->pos, F->vel, F->omega, dt, two_omega, bfecc, F->dep_b, F->dep_f, F->q0);
+    GGB_LAUNCHED();
+    k_resample<<<nb, kB, 0, s>>>(g, F->q0, F->dep_b, F->q0, 0, F->q1);
+    GGB_LAUNCHED();
+    if (bfecc) {
+        k_resample<<<nb, kB, 0, s>>>(g, F->q1, F->dep_f, F->q0, 1, F->q2);
+        GGB_LAUNCHED();
+    }
+    double relax = F->prm.forcing > 0 ? 1.0 - exp(-F->prm.forcing * dt) : 0.0;
+    k_limit_relax<<<nb, kB, 0, s>>>(g, t->pos, F->dep_b, F->q0, F->q2, bfecc, two_omega, relax, F->omega_band, F->q1,
+                                    F->omega);
+    GGB_LAUNCHED();
+    run_solve(F, Pv, 1, F->prm.cg_maxit);
+    launch_velocity(F, Pv);
+    sync();
+}
+
+GGB_EXPORT double fluid_max_speed(const Fluid *F) {
+    FluidPriv *Pv = priv_of(F);
+    cudaStream_t s = stream();
+    int n = F->cs->ncells;
+    GGB_CHECK(cudaMemsetAsync(Pv->vmax_bits, 0, sizeof(unsigned int), s));
+    k_max_speed2<<<blocks_for(n), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
+    GGB_LAUNCHED();
+    GGB_CHECK(cudaMemcpyAsync(Pv->vmax_host, Pv->vmax_bits, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaStreamSynchronize(s));
+    float m;
+    memcpy(&m, Pv->vmax_host, sizeof(m));
+    return sqrt((double)m);
+}

@@ -1,0 +1,115 @@
+// ggb_internal.h — host-side internals of libggb_cuda.so: error handling, the
+// library stream, allocation helpers, the launch counter and the private
+// device-side tables attached to every CubeSphere / Fluid / Render.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "cubesphere.h"
+#include "fluid.h"
+#include "particles.h"
+#include "render.h"
+#include "ggb_device.cuh"
+
+#define GGB_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace ggb {
+
+[[noreturn]] void fail_cuda(const char *what, cudaError_t e, const char *file, int line);
+[[noreturn]] void fail_msg(const char *fmt, ...);
+
+#define GGB_CHECK(x)                                                         \
+    do {                                                                     \
+        cudaError_t e_ = (x);                                                \
+        if (e_ != cudaSuccess) ::ggb::fail_cuda(#x, e_, __FILE__, __LINE__); \
+    } while (0)
+
+// Call after every kernel launch: counts it and surfaces launch errors.
+#define GGB_LAUNCHED()                                                                 \
+    do {                                                                               \
+        ::ggb::note_launch(1);                                                         \
+        cudaError_t e_ = cudaGetLastError();                                           \
+        if (e_ != cudaSuccess) ::ggb::fail_cuda("kernel launch", e_, __FILE__, __LINE__); \
+    } while (0)
+
+void note_launch(long k);
+long launch_count();
+
+// The stream every entry point issues its work on; created on first use for
+// the current device.  The batched API may redirect it while capturing.
+cudaStream_t stream();
+void set_stream(cudaStream_t s);
+void sync();
+int device_sm_count();
+// True when there is a usable CUDA device; entry points fail loudly otherwise.
+bool have_device();
+
+void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled
+void dev_free(void *p);
+void *managed_alloc(size_t bytes);  // cudaMallocManaged, zero-filled, resident on the device
+void managed_free(void *p);
+
+inline unsigned grid_for(size_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+// Face-tiled operator tables of one cubed-sphere grid (device memory).
+//   wslot[s*n + c], s = 0..3: weight of the link from cell c to its on-face
+//       neighbour at (+1,0) E, (0,+1) N, (+1,+1) NE, (-1,+1) NW (0 = no link).
+//       The opposite directions of c are read from the neighbour's slots,
+//       which hold the same (symmetric) weight.
+//   ring_nb / ring_w [r*8 + k]: links of boundary-ring cell r that leave the
+//       face (or the 3x3 box); -1 terminates.  Only ring cells have such links.
+struct GridTables {
+    int N = 0, n = 0, nring = 0;
+    double h = 0;
+    bool managed = false;
+    // upstream layout (managed memory for a public grid, device memory otherwise)
+    float *pos = nullptr, *area = nullptr, *w = nullptr, *elen = nullptr, *gc = nullptr;
+    unsigned char *nnb = nullptr;
+    int *nbr = nullptr;
+    // device-only
+    int *ghost = nullptr;
+    float *wslot = nullptr;
+    int *ring_nb = nullptr;
+    float *ring_w = nullptr;
+    float *dinv = nullptr;
+    double total_area = 0;
+    int asym_count = 0, open_cells = 0;
+
+    GridDev dev() const {
+        GridDev g;
+        g.N = N;
+        g.n = n;
+        g.h = h;
+        g.ghost = ghost;
+        return g;
+    }
+};
+
+inline int ring_count(int N) { return N == 1 ? 1 : 4 * N - 4; }
+
+// Builds every table of an N grid on the GPU (FP64 geometry).  With
+// managed = true the upstream-layout arrays are managed memory.  Returns 0, or
+// -1 with a message on stderr.
+int grid_build(GridTables *t, int N, bool managed);
+void grid_release(GridTables *t);
+
+// Registry: the private tables of a public CubeSphere, keyed by cs->pos.
+GridTables *grid_lookup(const CubeSphere *cs);  // fails loudly when unknown
+
+// Device copy of an argument that may live in pageable host memory: returns
+// a device-accessible pointer to `bytes` bytes equal to `src` (staging it
+// through `scratch` when needed).  copy_back() writes a staged buffer back.
+struct Staged {
+    void *dev = nullptr;
+    void *host = nullptr;
+    size_t bytes = 0;
+    bool owned = false;
+    ~Staged();
+};
+void stage_in(Staged &s, const void *src, size_t bytes);
+void stage_out(Staged &s, void *dst, size_t bytes);  // for an output buffer
+void stage_finish(Staged &s);                          // copies an output back to the host
+
+}  // namespace ggb

@@ -1,0 +1,52 @@
+// ggb_solver.h — device descriptors of the multigrid-preconditioned CG solve.
+#pragma once
+
+#include "ggb_stencil.cuh"
+
+namespace ggb {
+
+constexpr int kMaxLev = 12;
+
+// One multigrid level on the device.
+struct LevelDev {
+    StencilDev S;
+    const float *dinv;  // [n] 1 / sum of link weights
+    float *x;           // [n] iterate (pre-smoothed, then corrected)
+    float *xo;          // [n] V-cycle output of this level
+    float *b;           // [n] right-hand side (restricted residual)
+    float *r;           // [n] residual after the pre-smooth
+    // transfer to the next coarser level
+    const int *ptap;    // [4n] coarse taps of each cell of this level
+    const float *pw;    // [4n] their bilinear weights
+    const int *rstart;  // [n_coarse+1] rows of R = P^T
+    const int *ridx;    // fine cells of each row (ascending)
+    const float *rw;    // weights of each row
+};
+
+struct SolveResult {
+    int iters;
+    int status;      // 0 ok, 1 barrier timeout
+    double relres;
+    int r_final;     // which r buffer holds the final residual (0: r, 1: r2)
+    int pad;
+};
+
+struct SolveParams {
+    int nlev;            // >= 1 when multigrid, 0 for the Jacobi preconditioner
+    int nlev_grid;       // non-coarsest levels 0..nlev_grid-1 run grid-wide
+    int coarse_on_grid;  // coarsest level swept grid-wide (else by block 0)
+    int coarse_sweeps;   // Jacobi sweeps on the coarsest level (upstream: 60)
+    int remove_mean;     // project the mean out of omega first
+    int maxit;
+    double tol;
+    double total_area;
+    LevelDev L[kMaxLev];
+    const float *area;   // level-0 cell areas
+    float *omega, *psi;
+    float *r, *r2, *p, *p2, *Ap, *z;  // level-0 CG vectors (r / p ping-pong)
+    double *part;        // [5][gridDim.x] per-block partial sums
+    GridBarrier *bar;
+    SolveResult *res;
+};
+
+}  // namespace ggb

@@ -1,0 +1,149 @@
+// runtime.cu — error reporting, the library stream, allocation, argument
+// staging and the kernel-launch counter of libggb_cuda.so.
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+
+#include "ggb_internal.h"
+
+namespace ggb {
+
+void fail_cuda(const char *what, cudaError_t e, const char *file, int line) {
+    fprintf(stderr, "libggb_cuda: CUDA error in %s (%s:%d): %s\n", what, file, line, cudaGetErrorString(e));
+    fflush(stderr);
+    exit(1);
+}
+
+void fail_msg(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    fprintf(stderr, "libggb_cuda: ");
+    vfprintf(stderr, fmt, ap);
+    fprintf(stderr, "\n");
+    va_end(ap);
+    fflush(stderr);
+    exit(1);
+}
+
+static std::atomic<long> g_launches{0};
+void note_launch(long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+static std::mutex g_stream_mu;
+static cudaStream_t g_own_stream = nullptr;
+static cudaStream_t g_override = nullptr;
+static int g_sms = 0;
+
+bool have_device() {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+cudaStream_t stream() {
+    if (g_override) return g_override;
+    std::lock_guard<std::mutex> lk(g_stream_mu);
+    if (!g_own_stream) {
+        if (!have_device()) fail_msg("no CUDA device is available (this library has no CPU path)");
+        GGB_CHECK(cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking));
+    }
+    return g_own_stream;
+}
+
+void set_stream(cudaStream_t s) { g_override = s; }
+
+void sync() { GGB_CHECK(cudaStreamSynchronize(stream())); }
+
+int device_sm_count() {
+    if (!g_sms) {
+        int dev = 0;
+        GGB_CHECK(cudaGetDevice(&dev));
+        GGB_CHECK(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_sms;
+}
+
+void *dev_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (!bytes) bytes = 16;
+    GGB_CHECK(cudaMalloc(&p, bytes));
+    GGB_CHECK(cudaMemsetAsync(p, 0, bytes, stream()));
+    return p;
+}
+
+void dev_free(void *p) {
+    if (p) GGB_CHECK(cudaFree(p));
+}
+
+void *managed_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (!bytes) bytes = 16;
+    GGB_CHECK(cudaMallocManaged(&p, bytes, cudaMemAttachGlobal));
+    int dev = 0;
+    GGB_CHECK(cudaGetDevice(&dev));
+#if CUDART_VERSION >= 13000
+    cudaMemLocation loc;
+    loc.type = cudaMemLocationTypeDevice;
+    loc.id = dev;
+    cudaMemAdvise(p, bytes, cudaMemAdviseSetPreferredLocation, loc);
+    cudaMemPrefetchAsync(p, bytes, loc, 0, stream());
+#else
+    cudaMemAdvise(p, bytes, cudaMemAdviseSetPreferredLocation, dev);
+    cudaMemPrefetchAsync(p, bytes, dev, stream());
+#endif
+    cudaGetLastError();  // advice / prefetch are hints; ignore "not supported"
+    GGB_CHECK(cudaMemsetAsync(p, 0, bytes, stream()));
+    return p;
+}
+
+void managed_free(void *p) {
+    if (p) GGB_CHECK(cudaFree(p));
+}
+
+static bool device_accessible(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+Staged::~Staged() {
+    if (owned) cudaFree(dev);
+}
+
+void stage_in(Staged &s, const void *src, size_t bytes) {
+    s.bytes = bytes;
+    s.host = const_cast<void *>(src);
+    if (device_accessible(src)) {
+        s.dev = const_cast<void *>(src);
+        s.owned = false;
+        return;
+    }
+    GGB_CHECK(cudaMalloc(&s.dev, bytes ? bytes : 16));
+    s.owned = true;
+    GGB_CHECK(cudaMemcpyAsync(s.dev, src, bytes, cudaMemcpyHostToDevice, stream()));
+}
+
+void stage_out(Staged &s, void *dst, size_t bytes) {
+    s.bytes = bytes;
+    s.host = dst;
+    if (device_accessible(dst)) {
+        s.dev = dst;
+        s.owned = false;
+        return;
+    }
+    GGB_CHECK(cudaMalloc(&s.dev, bytes ? bytes : 16));
+    s.owned = true;
+}
+
+void stage_finish(Staged &s) {
+    if (s.owned) GGB_CHECK(cudaMemcpyAsync(s.host, s.dev, s.bytes, cudaMemcpyDeviceToHost, stream()));
+    sync();
+}
+
+}  // namespace ggb
+
+GGB_EXPORT long ggb_launch_count(void) { return ggb::launch_count(); }

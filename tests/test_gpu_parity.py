@@ -1,0 +1,349 @@
+"""Parity of the CUDA path (libggb_cuda.so, called through the C ABI) with the
+CPU restatement and the golden fixtures of the upstream build.
+
+Tolerances (stated per test):
+  * integer / index results (neighbour tables, point location, tap indices):
+    bit-exact;
+  * one-pass FP32 outputs computed in FP64 (positions, areas, weights,
+    operator applications): relative 1e-6 of the field's scale;
+  * results through the CG solve or several steps: relative L2 1e-4 against
+    the FP32 restatement (the CG / FP64 reductions sum in another order);
+  * face images of one deposit: the per-texel compositing order is the
+    upstream one, so every texel must agree to 1e-6 absolute.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import ggb_api as G
+import ggb_cases as K
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def scaled_max(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.max(np.abs(a - b), initial=0.0) / max(np.max(np.abs(b), initial=0.0), 1e-300)
+
+
+# ------------------------------------------------------------------ grid
+
+@pytest.mark.parametrize("N", [2, 3, 4, 8, 16, 33, 64, 128])
+def test_grid_tables(gpu, orc32, N):
+    t, o = K.grid_tables(gpu, N), K.grid_tables(orc32, N)
+    assert np.array_equal(t["nnb"], o["nnb"])
+    nb_t, w_t, e_t, g_t = K.sorted_links(t)
+    nb_o, w_o, e_o, g_o = K.sorted_links(o)
+    assert np.array_equal(nb_t, nb_o)                      # neighbour sets: bit-exact
+    assert scaled_max(t["pos"], o["pos"]) <= 1e-7
+    assert scaled_max(t["area"], o["area"]) <= 1e-6
+    assert scaled_max(w_t, w_o) <= 1e-6
+    assert scaled_max(e_t, e_o) <= 1e-6
+    assert scaled_max(g_t, g_o) <= 1e-6
+    assert abs(float(t["total_area"]) - 4 * np.pi) < 1e-4 * 4 * np.pi
+    assert int(t["asym_count"]) == int(o["asym_count"]) and int(t["open_cells"]) == int(o["open_cells"])
+
+
+@pytest.mark.parametrize("N", [8, 16])
+def test_grid_tables_golden(gpu, N):
+    t, gold = K.grid_tables(gpu, N), golden(f"grid_N{N}")
+    assert np.array_equal(t["nnb"], gold["nnb"])
+    assert np.array_equal(K.sorted_links(t)[0], K.sorted_links(gold)[0])
+    assert scaled_max(t["pos"], gold["pos"]) <= 1e-7
+
+
+def test_device_cell_of_is_bit_exact(gpu):
+    """Device point location on every cell centre and the 100k directions of
+    upstream tests/test_cubesphere.c equals the upstream host result."""
+    gold = golden("cellof_N64")
+    g = gpu.grid(64)
+    dirs = np.ascontiguousarray(K.lcg_dirs())
+    out = np.zeros(len(dirs), np.int32)
+    gpu.lib.ggb_cell_of_batch.argtypes = [C.POINTER(gpu.T["CubeSphere"]), C.POINTER(C.c_double), C.c_int,
+                                          C.POINTER(C.c_int)]
+    gpu.lib.ggb_cell_of_batch(C.byref(g.cs), dirs.ctypes.data_as(C.POINTER(C.c_double)), len(dirs),
+                              out.ctypes.data_as(C.POINTER(C.c_int)))
+    assert np.array_equal(out, gold["cells"])
+    cen = np.ascontiguousarray(g.arrays()["pos"].astype(np.float64))
+    out2 = np.zeros(g.n, np.int32)
+    gpu.lib.ggb_cell_of_batch(C.byref(g.cs), cen.ctypes.data_as(C.POINTER(C.c_double)), g.n,
+                              out2.ctypes.data_as(C.POINTER(C.c_int)))
+    assert np.array_equal(out2, np.arange(g.n))
+    # host entry point too
+    assert all(g.cell_of(d) == c for d, c in zip(dirs[:2000], gold["cells"][:2000]))
+    g.free()
+
+
+def test_device_taps_match_host(gpu, orc32):
+    """Bilinear taps incl. ghost taps across cube edges and corners."""
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(20000, 3))
+    # bias toward face edges / corners
+    d[:5000, 1] = d[:5000, 0] * (1 + 1e-3 * rng.normal(size=5000))
+    d[5000:8000, :] = np.sign(d[5000:8000, :]) * (1 + 1e-2 * rng.random((3000, 3)))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = np.ascontiguousarray(d)
+    g, go = gpu.grid(16), orc32.grid(16)
+    idx = np.zeros((len(d), 4), np.int32)
+    wt = np.zeros((len(d), 4), np.float64)
+    gpu.lib.ggb_taps_batch.argtypes = [C.POINTER(gpu.T["CubeSphere"]), C.POINTER(C.c_double), C.c_int,
+                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    gpu.lib.ggb_taps_batch(C.byref(g.cs), d.ctypes.data_as(C.POINTER(C.c_double)), len(d),
+                           idx.ctypes.data_as(C.POINTER(C.c_int)), wt.ctypes.data_as(C.POINTER(C.c_double)))
+    ri = np.zeros(4, np.int32)
+    rw = np.zeros(4, np.float64)
+    bad = 0
+    for k in range(len(d)):
+        orc32.lib.cs_taps(C.byref(go.cs), G.Vec3(*d[k]), ri.ctypes.data_as(C.POINTER(C.c_int)),
+                          rw.ctypes.data_as(C.POINTER(C.c_double)))
+        bad += not np.array_equal(ri, idx[k])
+        assert np.max(np.abs(rw - wt[k])) < 1e-12
+    assert bad == 0
+    g.free()
+    go.free()
+
+
+# ------------------------------------------------------------ operators
+
+@pytest.mark.parametrize("N", [16, 64])
+def test_operators(gpu, orc32, N):
+    a, b = K.operators(gpu, N), K.operators(orc32, N)
+    for k in a:
+        assert scaled_max(a[k], b[k]) <= 2e-6, k
+
+
+def test_operators_golden(gpu):
+    a, gold = K.operators(gpu, 16), golden("ops_N16")
+    for k in a:
+        assert scaled_max(a[k], gold[k]) <= 2e-6, k
+
+
+# ---------------------------------------------------------------- solve
+
+@pytest.mark.parametrize("N,multigrid", [(64, 1), (16, 1), (9, 1), (16, 0)])
+def test_poisson(gpu, orc32, N, multigrid):
+    def solve(api):
+        g = api.grid(N)
+        fs = G.FluidSim(api, g, cg_tol=1e-6, cg_maxit=5000, multigrid=multigrid)
+        pos = g.arrays()["pos"].astype(np.float64)
+        fs.field("omega")[:] = K.lap_exact(pos).astype(np.float32)
+        api.lib.fluid_remove_mean(C.byref(g.cs), fs.F.omega)
+        it = api.lib.fluid_solve_psi(C.byref(fs.F))
+        out = dict(psi=fs.field("psi").copy(), it=it, relres=fs.F.cg_relres, pos=pos)
+        fs.free()
+        g.free()
+        return out
+
+    a, b = solve(gpu), solve(orc32)
+    assert a["relres"] <= 1e-6
+    assert abs(a["it"] - b["it"]) <= 1
+    assert rel_l2(a["psi"], b["psi"]) < 1e-5
+    ex = K.psi_exact(a["pos"])
+    if N >= 64:
+        assert rel_l2(a["psi"], ex) < 0.02   # upstream tests/test_poisson.c:72
+
+
+def test_poisson_golden(gpu):
+    a, gold = K.poisson(gpu, 16), golden("poisson_N16")
+    assert int(a["iters"]) == int(gold["iters"])
+    assert rel_l2(a["psi"], gold["psi"]) < 1e-5
+    assert rel_l2(a["vel"], gold["vel"]) < 1e-5
+
+
+# ----------------------------------------------------------------- steps
+
+@pytest.mark.parametrize("bfecc", [1, 0])
+def test_short_run(gpu, orc32, bfecc):
+    g = orc32.grid(32)
+    vel0, vband = K.initial_velocity(orc32, g, seed=3)
+    g.free()
+    a = K.run(gpu, 32, 3000, 96, 5, vel0, vband, forcing=0.5, rotation=3.0, bfecc=bfecc)
+    b = K.run(orc32, 32, 3000, 96, 5, vel0, vband, forcing=0.5, rotation=3.0, bfecc=bfecc)
+    assert np.array_equal(a["cg"], b["cg"]) or np.max(np.abs(a["cg"] - b["cg"])) <= 1
+    assert np.max(np.abs(a["dts"] - b["dts"]) / b["dts"]) < 1e-5
+    for k in ("omega0", "psi0", "vel0", "omega", "psi", "vel"):
+        assert rel_l2(a[k], b[k]) < 1e-4, (k, rel_l2(a[k], b[k]))
+    ang = np.arccos(np.clip(np.sum(a["pos"] * b["pos"], 1) / np.linalg.norm(a["pos"], axis=1)
+                            / np.linalg.norm(b["pos"], axis=1), -1, 1))
+    assert np.median(ang) < 1e-6 and np.percentile(ang, 99) < 1e-5
+    assert np.max(np.abs(a["faces"] - b["faces"])) < 1e-3
+    assert np.mean(np.abs(a["faces"] - b["faces"])) < 1e-6
+
+
+def test_run_golden(gpu):
+    gold = golden("run_N16")
+    a = K.run(gpu, 16, 600, 40, 4, gold["vel_init"], gold["vband"])
+    for k in ("omega", "psi", "vel"):
+        assert rel_l2(a[k], gold[k]) < 1e-4, k
+    assert np.max(np.abs(a["pos"] - gold["pos"])) < 1e-5
+    assert np.max(np.abs(a["faces"] - gold["faces"])) < 1e-3
+
+
+def test_fp32_path_error_vs_fp64_oracle(gpu, orc64):
+    """psi / u / particle error of the FP32 GPU path against the FP64 oracle
+    (tol 1e-10) after 10 steps of fixed dt on N=32."""
+    g = orc64.grid(32)
+    v64, b64 = K.initial_velocity(orc64, g, seed=2)
+    g.free()
+    h = (np.pi / 2) / 32
+    a = K.run(gpu, 32, 2000, 64, 10, v64.astype(np.float32), b64.astype(np.float32), tol=1e-6, fixed_dt=h / 2)
+    b = K.run(orc64, 32, 2000, 64, 10, v64, b64, tol=1e-10, fixed_dt=h / 2)
+    assert rel_l2(a["psi"], b["psi"]) < 1e-4
+    assert rel_l2(a["vel"], b["vel"]) < 1e-4
+
+
+# ---------------------------------------------------------------- render
+
+def test_deposit_golden_exact_order(gpu):
+    gold = golden("deposit_R48")
+    a = K.deposit(gpu, 48, gold["prev"], gold["pos"], gold["col"], fade_steps=3)
+    diff = np.abs(a["faces"] - gold["faces"])
+    assert np.max(diff) <= 1e-6
+    assert float(a["g"]) == float(gold["g"])
+
+
+@pytest.mark.parametrize("R,radius,max_angle,n", [(64, 1.0, 0.05, 3000), (50, 2.5, 0.05, 1500),
+                                                  (40, 0.5, 0.6, 300), (33, 1.0, 3.0, 40), (96, 1.0, 0.01, 0)])
+def test_deposit_cases(gpu, orc32, R, radius, max_angle, n):
+    """Edge cases: ragged tiles (R not a multiple of 32), wide splats, the
+    0.75 radius clamp, long arcs (many samples, many tiles), no particles."""
+    prev, pos, col = K.random_arcs(n, seed=R, max_angle=max_angle)
+    a = K.deposit(gpu, R, prev, pos, col, radius=radius)
+    b = K.deposit(orc32, R, prev, pos, col, radius=radius)
+    assert np.max(np.abs(a["faces"] - b["faces"]), initial=0.0) <= 1e-6
+
+
+def test_deposit_dense_tile_sorts_in_global_memory(gpu, orc32):
+    """> 2048 particles in one tile (the global-memory sort path)."""
+    rng = np.random.default_rng(11)
+    n = 6000
+    c = np.array([0.0, 0.0, 1.0])
+    prev = c + 0.01 * rng.normal(size=(n, 3))
+    prev /= np.linalg.norm(prev, axis=1, keepdims=True)
+    pos = prev + 0.002 * rng.normal(size=(n, 3))
+    pos /= np.linalg.norm(pos, axis=1, keepdims=True)
+    col = rng.uniform(0.1, 1, size=(n, 4))
+    a = K.deposit(gpu, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    b = K.deposit(orc32, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
+
+
+def test_fade_renormalisation(gpu, orc32):
+    """g falls below 1e-4 (the buffer is rescaled, fused into the next deposit)."""
+    prev, pos, col = K.random_arcs(500, seed=5, max_angle=0.05)
+    for steps in (460, 465):
+        a = K.deposit(gpu, 40, prev, pos, col, fade_steps=steps)
+        b = K.deposit(orc32, 40, prev, pos, col, fade_steps=steps)
+        assert float(a["g"]) == float(b["g"])
+        assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
+
+
+def test_render_read_back_api(gpu, orc32):
+    """render_texel / render_sample_dir / render_pixel8 against the restatement."""
+    prev, pos, col = K.random_arcs(2000, seed=9, max_angle=0.1)
+    out = {}
+    for name, api in (("gpu", gpu), ("orc", orc32)):
+        ps = G.ParticleSet(api, len(prev))
+        ps.array("prev", 3)[:] = prev
+        ps.array("pos", 3)[:] = pos
+        ps.array("col", 4)[:] = col
+        sp = G.Splat(api, 32)
+        sp.fade(0.02)
+        sp.deposit(ps)
+        tex = np.zeros(4, np.float32)
+        texels = []
+        for f in range(6):
+            for (x, y) in ((0, 0), (5, 7), (31, 31), (16, 3)):
+                api.lib.render_texel(C.byref(sp.r), f, x, y, api.ptr(tex))
+                texels.append(tex.copy())
+        samples = []
+        rng = np.random.default_rng(1)
+        for d in rng.normal(size=(200, 3)):
+            api.lib.render_sample_dir(C.byref(sp.r), *map(float, d), api.ptr(tex))
+            samples.append(tex.copy())
+        px = np.zeros(4, np.uint8)
+        pix = []
+        for t in texels:
+            tt = np.ascontiguousarray(t)
+            api.lib.render_pixel8(api.ptr(tt), None, px.ctypes.data_as(C.POINTER(C.c_ubyte)))
+            pix.append(px.copy())
+        out[name] = (np.array(texels), np.array(samples), np.array(pix))
+        sp.free()
+        ps.free()
+    for x, y in zip(out["gpu"], out["orc"]):
+        assert np.max(np.abs(x.astype(np.float64) - y)) <= (1 if x.dtype == np.uint8 else 1e-6)
+
+
+# -------------------------------------------------------------- particles
+
+def test_particles_init_and_colour(gpu, orc32):
+    img = __import__("ggb_inputs").strip(4)
+    res = {}
+    for name, api in (("gpu", gpu), ("orc", orc32)):
+        ps = G.ParticleSet(api, 50000)
+        ps.colour(img)
+        res[name] = (ps.array("pos", 3).copy(), ps.array("col", 4).copy())
+        ps.free()
+    assert np.max(np.abs(res["gpu"][0] - res["orc"][0])) <= 1e-7
+    assert np.max(np.abs(res["gpu"][1] - res["orc"][1])) <= 1e-6
+
+
+def test_solid_body_rotation(gpu):
+    """upstream tests/test_flow.c: one revolution of solid-body rotation."""
+    g = gpu.grid(64)
+    pos = g.arrays()["pos"].astype(np.float64)
+    vel0 = np.cross(np.array([0.0, 1.0, 0.0]), pos).astype(np.float32).ravel()
+    fs = G.FluidSim(gpu, g, bfecc=1, cg_tol=1e-6, cg_maxit=2000)
+    fs.set_state(vel0)
+    area = g.arrays()["area"].astype(np.float64)
+    v = fs.field("vel", 3).reshape(-1, 3).astype(np.float64)
+    v0 = vel0.reshape(-1, 3)
+    vrel = np.sqrt(np.sum(np.sum((v - v0) ** 2, 1) * area) / np.sum(np.sum(v0 ** 2, 1) * area))
+    assert vrel < 0.01
+    om0 = fs.field("omega").copy().astype(np.float64)
+    ex = 2 * pos[:, 1]
+    assert np.sqrt(np.sum((om0 - ex) ** 2 * area) / np.sum(ex ** 2 * area)) < 0.01
+    ps = G.ParticleSet(gpu, 5000)
+    start = ps.array("pos", 3).copy()
+    steps, dt = 400, 2 * np.pi / 400
+    for _ in range(steps):
+        ps.advect(g, fs.F.vel, dt)
+        fs.step(dt)
+    end = ps.array("pos", 3).astype(np.float64)
+    ang = np.arccos(np.clip(np.sum(end * start, 1) / np.linalg.norm(end, axis=1) / np.linalg.norm(start, axis=1),
+                            -1, 1))
+    assert ang.max() < g.cs.h
+    om = fs.field("omega").astype(np.float64)
+    assert np.sqrt(np.sum((om - om0) ** 2 * area) / np.sum(om0 ** 2 * area)) < 0.02
+    ps.free()
+    fs.free()
+    g.free()
+
+
+def test_initial_velocity_kernel(gpu, orc32):
+    g, go = gpu.grid(32), orc32.grid(32)
+    a = K.initial_velocity(gpu, g, seed=7, bands=12)
+    b = K.initial_velocity(orc32, go, seed=7, bands=12)
+    for x, y in zip(a, b):
+        assert scaled_max(x, y) < 1e-6
+    g.free()
+    go.free()
+
+
+def test_host_pointer_operands(gpu, orc32):
+    """Operators called with pageable host buffers are staged, not run on the CPU."""
+    n0 = gpu.lib.ggb_launch_count()
+    K.operators(gpu, 16)
+    assert gpu.lib.ggb_launch_count() > n0
