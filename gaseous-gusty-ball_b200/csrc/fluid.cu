@@ -14,6 +14,7 @@
 namespace ggb {
 
 int pcg_grid_size();
+int pcg_max_blocks();
 int pcg_block_size();
 void pcg_launch(const SolveParams &prm, cudaStream_t s);
 
@@ -186,7 +187,7 @@ __global__ void k_ptaps(int nf, const float *fine_pos, GridDev coarse, int *ptap
         for (int k = 0; k < 4; k++) {
             ptap[4 * i + k] = idx[k];
             pw[4 * i + k] = (float)wt[k];
-            atomicAdd(rcount + idx[k] + 1, 1);
+            atomicAdd(rcount + idx[k], 1);  // row counts; exclusive scan gives the row starts
         }
     }
 }
@@ -333,7 +334,7 @@ static void build_levels(Fluid *F, FluidPriv *Pv) {
     }
 }
 
-constexpr int kBlockLevelMax = 6144;  // levels up to N=32 run inside one block
+constexpr int kBlockLevelMax = 1536;  // levels up to N=16 run inside one block (shared memory)
 
 static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
     SolveParams P;
@@ -387,13 +388,19 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
     return P;
 }
 
+void solve_trace_target(unsigned long long **buf, int *cap);
+
 // Launch the solve and read back its result into F (sync).
 static int run_solve(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
     SolveParams P = solve_params(F, Pv, remove_mean, maxit);
+    solve_trace_target(&P.trace, &P.trace_cap);
     cudaStream_t s = stream();
+    stage_begin(ST_SOLVE);
     pcg_launch(P, s);
+    stage_end(ST_SOLVE);
     GGB_CHECK(cudaMemcpyAsync(Pv->res_host, Pv->res, sizeof(SolveResult), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaStreamSynchronize(s));
+    stage_collect();
     const SolveResult &R = *Pv->res_host;
     if (R.status != 0) fail_msg("Poisson solve aborted: a grid barrier timed out");
     F->cg_iters = R.iters;
@@ -486,7 +493,7 @@ GGB_EXPORT int fluid_init(Fluid *F, const CubeSphere *cs, const FluidParams *prm
         Pv->lr[0] = (float *)dev_alloc(sizeof(float) * n);
         F->nlev = 0;
     }
-    Pv->part = (double *)dev_alloc(sizeof(double) * 8 * pcg_grid_size());
+    Pv->part = (double *)dev_alloc(sizeof(double) * 8 * pcg_max_blocks());
     Pv->wpart = (double *)dev_alloc(sizeof(double) * 1024);
     Pv->bar = (GridBarrier *)dev_alloc(sizeof(GridBarrier));
     Pv->res = (SolveResult *)dev_alloc(sizeof(SolveResult));
@@ -539,8 +546,10 @@ GGB_EXPORT int fluid_solve_psi(Fluid *F) {
 
 static void launch_velocity(Fluid *F, FluidPriv *Pv) {
     const GridTables *t = Pv->grid0;
+    stage_begin(ST_VELOCITY);
     k_velocity<<<blocks_for(t->n), kB, 0, stream()>>>(t->n, t->pos, t->nnb, t->nbr, t->gc, F->psi, F->vel);
     GGB_LAUNCHED();
+    stage_end(ST_VELOCITY);
 }
 
 GGB_EXPORT void fluid_compute_velocity(Fluid *F) {
@@ -578,6 +587,7 @@ GGB_EXPORT void fluid_step(Fluid *F, double dt) {
     int bfecc = F->prm.bfecc != 0;
     GridDev g = t->dev();
     unsigned nb = blocks_for(t->n);
+    stage_begin(ST_ADVECT);
     k_departures<<<nb, kB, 0, s>>>(g, t->pos, F->vel, F->omega, dt, two_omega, bfecc, F->dep_b, F->dep_f, F->q0);
     GGB_LAUNCHED();
     k_resample<<<nb, kB, 0, s>>>(g, F->q0, F->dep_b, F->q0, 0, F->q1);
@@ -590,6 +600,7 @@ GGB_EXPORT void fluid_step(Fluid *F, double dt) {
     k_limit_relax<<<nb, kB, 0, s>>>(g, t->pos, F->dep_b, F->q0, F->q2, bfecc, two_omega, relax, F->omega_band, F->q1,
                                     F->omega);
     GGB_LAUNCHED();
+    stage_end(ST_ADVECT);
     run_solve(F, Pv, 1, F->prm.cg_maxit);
     launch_velocity(F, Pv);
     sync();
@@ -599,12 +610,16 @@ GGB_EXPORT double fluid_max_speed(const Fluid *F) {
     FluidPriv *Pv = priv_of(F);
     cudaStream_t s = stream();
     int n = F->cs->ncells;
+    stage_begin(ST_MAXSPEED);
     GGB_CHECK(cudaMemsetAsync(Pv->vmax_bits, 0, sizeof(unsigned int), s));
     k_max_speed2<<<blocks_for(n), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
     GGB_LAUNCHED();
+    stage_end(ST_MAXSPEED);
     GGB_CHECK(cudaMemcpyAsync(Pv->vmax_host, Pv->vmax_bits, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaStreamSynchronize(s));
+    stage_collect();
     float m;
     memcpy(&m, Pv->vmax_host, sizeof(m));
     return sqrt((double)m);
 }
+

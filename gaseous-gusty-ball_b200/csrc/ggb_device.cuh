@@ -159,9 +159,11 @@ __device__ __forceinline__ void taps(const GridDev &g, D3 p, int idx[4], double 
     int f;
     double x, y;
     locate(p, g.h, f, x, y);
-    int i0 = (int)floor(x), j0 = (int)floor(y);
-    double fx = x - i0, fy = y - j0;
     int N = g.N;
+    // x, y lie in [-0.5, N-0.5] for any unit vector; the clamp only guards the
+    // table reads against non-finite input
+    int i0 = clampi((int)floor(x), -1, N - 1), j0 = clampi((int)floor(y), -1, N - 1);
+    double fx = x - i0, fy = y - j0;
     if (i0 >= 0 && j0 >= 0 && i0 + 1 < N && j0 + 1 < N) {
         int b = (f * N + j0) * N + i0;
         idx[0] = b;
@@ -230,7 +232,17 @@ __device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) 
 }
 __device__ __forceinline__ int ld_volatile_i32(const int *p) { return *(volatile const int *)p; }
 
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Returns true when all blocks arrived; false on timeout or an earlier error.
+// Arrival is an acq_rel atomic of thread 0 after a block barrier (so every
+// write of the block before the barrier is released); the last block resets
+// the counter and releases the generation; the others poll it with acquire
+// loads.  The timeout is checked every 64 polls.
 __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
     __shared__ int s_ok;
     __syncthreads();
@@ -238,28 +250,27 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
         int ok = ld_volatile_i32(&bar->err) == 0;
         if (ok) {
             unsigned int g = ld_acquire_u32(&bar->gen);
-            __threadfence();
-            unsigned int arrived = atomicAdd(&bar->count, 1u);
+            unsigned int arrived = atom_add_acq_rel_u32(&bar->count, 1u);
             if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
-                atomicExch(&bar->count, 0u);
-                __threadfence();
+                bar->count = 0;
                 st_release_u32(&bar->gen, g + 1);
             } else {
                 unsigned long long t0 = globaltimer_ns();
+                unsigned int polls = 0;
                 while (ld_acquire_u32(&bar->gen) == g) {
-                    if (ld_volatile_i32(&bar->err) != 0) {
-                        ok = 0;
-                        break;
+                    if ((++polls & 63u) == 0) {
+                        if (ld_volatile_i32(&bar->err) != 0) {
+                            ok = 0;
+                            break;
+                        }
+                        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                            atomicExch(&bar->err, 1);
+                            ok = 0;
+                            break;
+                        }
                     }
-                    if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-                        atomicExch(&bar->err, 1);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(40);
                 }
             }
-            __threadfence();  // acquire side: later loads of this block see the other blocks' writes
         }
         s_ok = ok;
     }

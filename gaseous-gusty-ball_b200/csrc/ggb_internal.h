@@ -46,6 +46,12 @@ int device_sm_count();
 // True when there is a usable CUDA device; entry points fail loudly otherwise.
 bool have_device();
 
+// Optional per-stage CUDA-event timing on the library stream (off by default).
+enum Stage { ST_PARTICLES = 0, ST_ADVECT, ST_SOLVE, ST_VELOCITY, ST_MAXSPEED, ST_BIN, ST_TILES, ST_N };
+void stage_begin(int s);
+void stage_end(int s);
+void stage_collect();  // after a stream sync: accumulate the recorded intervals
+
 void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled
 void dev_free(void *p);
 void *managed_alloc(size_t bytes);  // cudaMallocManaged, zero-filled, resident on the device

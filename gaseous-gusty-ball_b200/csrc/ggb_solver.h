@@ -44,7 +44,9 @@ struct SolveParams {
     const float *area;   // level-0 cell areas
     float *omega, *psi;
     float *r, *r2, *p, *p2, *Ap, *z;  // level-0 CG vectors (r / p ping-pong)
-    double *part;        // [5][gridDim.x] per-block partial sums
+    double *part;        // [RED_N][gridDim.x] per-block partial sums
+    unsigned long long *trace;  // optional: block 0 stamps %globaltimer at phase marks
+    int trace_cap;
     GridBarrier *bar;
     SolveResult *res;
 };

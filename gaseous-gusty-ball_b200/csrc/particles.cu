@@ -76,8 +76,10 @@ __global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *v
 
 void particles_advect_launch(int n, const GridDev &g, const float *vel, double dt, float *pos, float *prev,
                              cudaStream_t s) {
+    stage_begin(ST_PARTICLES);
     k_advect<<<blocks_for(n), kPB, 0, s>>>(n, g, vel, dt, pos, prev);
     GGB_LAUNCHED();
+    stage_end(ST_PARTICLES);
 }
 
 }  // namespace ggb

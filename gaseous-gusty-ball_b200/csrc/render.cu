@@ -142,7 +142,7 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
         D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
         arc_tiles(C, a, b, [&](int t) {
             unsigned slot = atomicAdd(tile_fill + t, 1u);
-            list[tile_start[t] + slot] = (unsigned)i;
+            if (tile_start[t] + slot < tile_start[t + 1]) list[tile_start[t] + slot] = (unsigned)i;
         });
     }
 }
@@ -294,7 +294,8 @@ __global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *prev,
     __syncthreads();
 
     const float rad = C.rad, invrad = C.invrad, invg = C.invg;
-    const int fpmax = (2 * (int)ceilf(rad)) * (2 * (int)ceilf(rad));
+    // texels with positive tent weight per axis: < 2 rad + 1 (rounding of invrad included)
+    const int fpmax = (2 * (int)ceilf(rad) + 1) * (2 * (int)ceilf(rad) + 1);
     const int win = max(1, min(kSampleCap, kEntryCap / max(1, fpmax)));
 
     for (int c0 = 0; c0 < cnt; c0 += kChunk) {
@@ -471,6 +472,7 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
+    stage_begin(ST_BIN);
     GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
     unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
@@ -482,6 +484,7 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     GGB_LAUNCHED();
     (void)sync_total;
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    stage_end(ST_BIN);
     GGB_CHECK(cudaStreamSynchronize(s));
     size_t need = *Pv->total_host;
     if (need > Pv->list_cap) {
@@ -489,6 +492,7 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
         Pv->list_cap = need + need / 4 + 1024;
         Pv->list = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->list_cap);
     }
+    stage_begin(ST_TILES);
     if (n > 0) {
         k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->list);
         GGB_LAUNCHED();
@@ -496,6 +500,7 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     k_rd_tiles<<<Pv->ntiles, kTB, sizeof(TileSmem), s>>>(C, P->prev, P->pos, P->col, Pv->tile_start, Pv->list,
                                                            r->buf);
     GGB_LAUNCHED();
+    stage_end(ST_TILES);
     Pv->pending = false;
     Pv->pending_scale = 1.f;
     Pv->dev_gen++;

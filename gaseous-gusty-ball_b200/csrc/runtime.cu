@@ -53,7 +53,41 @@ cudaStream_t stream() {
 
 void set_stream(cudaStream_t s) { g_override = s; }
 
-void sync() { GGB_CHECK(cudaStreamSynchronize(stream())); }
+void sync() {
+    GGB_CHECK(cudaStreamSynchronize(stream()));
+    stage_collect();
+}
+
+// ---- stage timing
+static bool g_timing = false;
+static cudaEvent_t g_ev[ST_N][2];
+static bool g_pending[ST_N];
+static double g_stage_ms[ST_N];
+static long g_stage_n[ST_N];
+
+void stage_begin(int s) {
+    if (!g_timing) return;
+    GGB_CHECK(cudaEventRecord(g_ev[s][0], stream()));
+}
+
+void stage_end(int s) {
+    if (!g_timing) return;
+    GGB_CHECK(cudaEventRecord(g_ev[s][1], stream()));
+    g_pending[s] = true;
+}
+
+void stage_collect() {
+    if (!g_timing) return;
+    for (int s = 0; s < ST_N; s++)
+        if (g_pending[s]) {
+            float ms = 0;
+            GGB_CHECK(cudaEventSynchronize(g_ev[s][1]));
+            GGB_CHECK(cudaEventElapsedTime(&ms, g_ev[s][0], g_ev[s][1]));
+            g_stage_ms[s] += ms;
+            g_stage_n[s]++;
+            g_pending[s] = false;
+        }
+}
 
 int device_sm_count() {
     if (!g_sms) {
@@ -147,3 +181,55 @@ void stage_finish(Staged &s) {
 }  // namespace ggb
 
 GGB_EXPORT long ggb_launch_count(void) { return ggb::launch_count(); }
+
+// Selects the CUDA device this library uses (before any other call).
+GGB_EXPORT int ggb_set_device(int dev) { return cudaSetDevice(dev) == cudaSuccess ? 0 : -1; }
+
+// Waits for all work issued by this library.
+GGB_EXPORT void ggb_sync(void) { ggb::sync(); }
+
+// Per-stage timing: enable/disable (resets the totals); read totals in ms and
+// interval counts for the stages particles, advect, solve, velocity,
+// max_speed, render binning, render tiles.
+GGB_EXPORT void ggb_stage_timing(int on) {
+    using namespace ggb;
+    sync();
+    if (on && !g_timing)
+        for (int s = 0; s < ST_N; s++) {
+            GGB_CHECK(cudaEventCreate(&g_ev[s][0]));
+            GGB_CHECK(cudaEventCreate(&g_ev[s][1]));
+        }
+    for (int s = 0; s < ST_N; s++) {
+        g_stage_ms[s] = 0;
+        g_stage_n[s] = 0;
+        g_pending[s] = false;
+    }
+    g_timing = on != 0;
+}
+
+GGB_EXPORT int ggb_stage_times(double *ms, long *count, int n) {
+    using namespace ggb;
+    sync();
+    for (int s = 0; s < ST_N && s < n; s++) {
+        ms[s] = g_stage_ms[s];
+        count[s] = g_stage_n[s];
+    }
+    return ST_N;
+}
+
+// Wall-clock interval of the library stream measured with CUDA events.
+static cudaEvent_t g_t0 = nullptr, g_t1 = nullptr;
+GGB_EXPORT void ggb_timer_start(void) {
+    if (!g_t0) {
+        GGB_CHECK(cudaEventCreate(&g_t0));
+        GGB_CHECK(cudaEventCreate(&g_t1));
+    }
+    GGB_CHECK(cudaEventRecord(g_t0, ggb::stream()));
+}
+GGB_EXPORT double ggb_timer_stop(void) {
+    GGB_CHECK(cudaEventRecord(g_t1, ggb::stream()));
+    GGB_CHECK(cudaEventSynchronize(g_t1));
+    float ms = 0;
+    GGB_CHECK(cudaEventElapsedTime(&ms, g_t0, g_t1));
+    return ms;
+}
