@@ -11,6 +11,7 @@
 #include "fluid.h"
 #include "particles.h"
 #include "render.h"
+#include "ggb_ext.h"
 #include "ggb_device.cuh"
 
 #define GGB_EXPORT extern "C" __attribute__((visibility("default")))

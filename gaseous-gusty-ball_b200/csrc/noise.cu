@@ -160,15 +160,6 @@ GGB_EXPORT vec3 curl_noise(const Noise *nz, vec3 p, const CurlParams *cp) {
 
 // ---- additive: initial velocity on the GPU
 
-extern "C" {
-typedef struct {
-    int bands;
-    double band_amp;
-    double noise_amp, noise_scale, noise_lacunarity, noise_gain;
-    int noise_octaves;
-    unsigned int seed;
-} GGBInitParams;
-}
 
 // vel / vband: [ncells*3] (host or device memory).  Same field as the
 // application driver's initial_velocity (upstream src/main.c:321-351).

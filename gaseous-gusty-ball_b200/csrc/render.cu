@@ -39,6 +39,8 @@ struct RenderPriv {
     unsigned *tile_count = nullptr, *tile_start = nullptr, *tile_fill = nullptr;
     unsigned *list = nullptr;
     size_t list_cap = 0;
+    unsigned *slow_tiles = nullptr;  // tiles left to the sorted path
+    unsigned *slow_count = nullptr;
     unsigned *total_host = nullptr;
     bool pending = false;
     float pending_scale = 1.f;
@@ -129,10 +131,61 @@ __device__ __forceinline__ void arc_tiles(const SplatCfg &C, D3 a, D3 b, Emit em
             for (int tx = tlo[f][0]; tx <= thi[f][0]; tx++) emit((f * C.ntx + ty) * C.ntx + tx);
 }
 
+// Conservative tile set of an arc for binning (a superset of arc_tiles).  The
+// samples are normalised chord points of the great-circle arc a -> b; on a
+// face whose hemisphere holds both endpoints the gnomonic image of that arc is
+// the segment between the endpoint images, so the bounding box of the two
+// endpoint footprints (plus a margin) covers every sample footprint.  A face
+// is skipped when neither endpoint is near it: along an arc of angle theta,
+// d.c exceeds the larger endpoint value by at most a factor 1/cos(theta/2),
+// so no sample reaches d.c >= 0.5.  Long arcs and arcs leaving a face's
+// hemisphere take the exact per-sample path.
+template <class Emit>
+__device__ __forceinline__ void arc_tiles_bound(const SplatCfg &C, D3 a, D3 b, Emit emit) {
+    // FP32 is enough for a bound: the projections carry a 0.05-texel margin
+    // and the face test a 1e-3 margin, far above FP32 rounding.
+    const float ax = (float)a.x, ay = (float)a.y, az = (float)a.z, bx = (float)b.x, by = (float)b.y, bz = (float)b.z;
+    const float la = sqrtf(ax * ax + ay * ay + az * az), lb = sqrtf(bx * bx + by * by + bz * bz);
+    const float cth = (ax * bx + ay * by + az * bz) / (la * lb);
+    if (!(cth > 0.9f)) {  // theta > ~0.45 rad (or degenerate input): exact path
+        arc_tiles(C, a, b, emit);
+        return;
+    }
+    const float half_cos = sqrtf(0.5f * (1.0f + cth));  // cos(theta / 2)
+    const float Rf = (float)C.R;
+    for (int f = 0; f < 6; f++) {
+        float ca, ra, ua, cb, rb, ub;
+        switch (f) {
+            case 0: ca = az; ra = ax; ua = ay; cb = bz; rb = bx; ub = by; break;
+            case 1: ca = ax; ra = -az; ua = ay; cb = bx; rb = -bz; ub = by; break;
+            case 2: ca = -az; ra = -ax; ua = ay; cb = -bz; rb = -bx; ub = by; break;
+            case 3: ca = -ax; ra = az; ua = ay; cb = -bx; rb = bz; ub = by; break;
+            case 4: ca = ay; ra = ax; ua = -az; cb = by; rb = bx; ub = -bz; break;
+            default: ca = -ay; ra = ax; ua = az; cb = -by; rb = bx; ub = bz; break;
+        }
+        if (fmaxf(ca / la, cb / lb) < 0.5f * half_cos - 1e-3f) continue;
+        if (ca <= 0.05f * la || cb <= 0.05f * lb) {
+            // rare: an endpoint near or behind the face's horizon; exact samples for this arc
+            arc_tiles(C, a, b, emit);
+            return;
+        }
+        float pxa = (ra / ca + 1.0f) * 0.5f * Rf - 0.5f, pya = (1.0f - ua / ca) * 0.5f * Rf - 0.5f;
+        float pxb = (rb / cb + 1.0f) * 0.5f * Rf - 0.5f, pyb = (1.0f - ub / cb) * 0.5f * Rf - 0.5f;
+        float m = C.rad + 0.05f;
+        float x0 = fminf(pxa, pxb) - m, x1 = fmaxf(pxa, pxb) + m;
+        float y0 = fminf(pya, pyb) - m, y1 = fmaxf(pya, pyb) + m;
+        if (x1 < 0.f || y1 < 0.f || x0 > Rf - 1.f || y0 > Rf - 1.f) continue;
+        int tx0 = max(0, (int)floorf(x0)) / kT, tx1 = min(C.R - 1, (int)floorf(x1)) / kT;
+        int ty0 = max(0, (int)floorf(y0)) / kT, ty1 = min(C.R - 1, (int)floorf(y1)) / kT;
+        for (int ty = ty0; ty <= ty1; ty++)
+            for (int tx = tx0; tx <= tx1; tx++) emit((f * C.ntx + ty) * C.ntx + tx);
+    }
+}
+
 __global__ void k_rd_count(int n, SplatCfg C, const float *prev, const float *pos, unsigned *tile_count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
-        arc_tiles(C, a, b, [&](int t) { atomicAdd(tile_count + t, 1u); });
+        arc_tiles_bound(C, a, b, [&](int t) { atomicAdd(tile_count + t, 1u); });
     }
 }
 
@@ -140,7 +193,7 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
                           unsigned *tile_fill, unsigned *list) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
-        arc_tiles(C, a, b, [&](int t) {
+        arc_tiles_bound(C, a, b, [&](int t) {
             unsigned slot = atomicAdd(tile_fill + t, 1u);
             if (tile_start[t] + slot < tile_start[t + 1]) list[tile_start[t] + slot] = (unsigned)i;
         });
@@ -252,10 +305,12 @@ struct TileSmem {
 
 // One block per tile; see the file comment.
 __global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *prev, const float *pos, const float *col,
-                                                  const unsigned *tile_start, unsigned *list, float *buf) {
+                                                  const unsigned *tile_start, unsigned *list, float *buf,
+                                                  const unsigned *tiles, const unsigned *ntiles_p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
-    const int tile = blockIdx.x;
+    if (blockIdx.x >= *ntiles_p) return;
+    const int tile = (int)tiles[blockIdx.x];
     const int R = C.R, ntx = C.ntx;
     const int f = tile / (ntx * ntx), rem = tile - f * ntx * ntx, ty = rem / ntx, tx = rem - ty * ntx;
     const int x0 = tx * kT, y0 = ty * kT;
@@ -436,6 +491,139 @@ __global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *prev,
     }
 }
 
+// ---- fast per-tile path ------------------------------------------------
+// One pass over the tile's particles expands each arc's samples on this tile
+// (FP64, as upstream) and drops every (sample, texel) pair with positive tent
+// weight straight into that texel's fixed-size entry slots.  Each entry
+// carries the sample's global order key (particle index, k), and each texel
+// sorts its few entries by that key before blending, so neither the tile's
+// particle list nor the samples need any order.  A tile whose particles,
+// samples or per-texel entries exceed the fixed buffers is left untouched and
+// queued for k_rd_tiles (the sorted, windowed path).
+constexpr int kFastParticles = 512;
+constexpr int kFastSamples = 1536;
+constexpr int kTexelSlots = 12;
+
+struct FastSmem {
+    float4 col[kFastParticles];
+    float2 spos[kFastSamples];
+    unsigned long long skey[kFastSamples];
+    unsigned short sslot[kFastSamples];
+    unsigned short ent[kT * kT * kTexelSlots];
+    int tcnt[kT * kT];
+    int nsamp, overflow;
+};
+
+__global__ void __launch_bounds__(kTB) k_rd_tiles_fast(SplatCfg C, const float *prev, const float *pos,
+                                                       const float *col, const unsigned *tile_start,
+                                                       const unsigned *list, float *buf, unsigned *slow_tiles,
+                                                       unsigned *slow_count) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastSmem &S = *reinterpret_cast<FastSmem *>(smem_raw);
+    const int tile = blockIdx.x;
+    const int R = C.R, ntx = C.ntx;
+    const int f = tile / (ntx * ntx), rem = tile - f * ntx * ntx, ty = rem / ntx, tx = rem - ty * ntx;
+    const int x0 = tx * kT, y0 = ty * kT;
+    const int tw = min(kT, R - x0), th = min(kT, R - y0);
+    const unsigned lstart = tile_start[tile];
+    const int cnt = (int)(tile_start[tile + 1] - lstart);
+    if (cnt == 0 && !C.renorm) return;
+    if (cnt > kFastParticles) {
+        if (threadIdx.x == 0) slow_tiles[atomicAdd(slow_count, 1u)] = (unsigned)tile;
+        return;
+    }
+    if (threadIdx.x == 0) {
+        S.nsamp = 0;
+        S.overflow = 0;
+    }
+    for (int q = threadIdx.x; q < kT * kT; q += kTB) S.tcnt[q] = 0;
+    __syncthreads();
+    const float rad = C.rad, invrad = C.invrad, invg = C.invg;
+    for (int u = threadIdx.x; u < cnt; u += kTB) {
+        unsigned pidx = list[lstart + u];
+        D3 a = load3(prev + 3 * (size_t)pidx), b = load3(pos + 3 * (size_t)pidx);
+        S.col[u] = reinterpret_cast<const float4 *>(col)[pidx];
+        int ns = arc_samples(a, b, C.spacing);
+        for (int k = 1; k <= ns; k++) {
+            float px, py;
+            if (!face_px(f, arc_point(a, b, k, ns), R, px, py)) continue;
+            Box bx = footprint(px, py, rad, R);
+            int xa = max(bx.xlo, x0), xb = min(bx.xhi, x0 + tw - 1);
+            int ya = max(bx.ylo, y0), yb = min(bx.yhi, y0 + th - 1);
+            if (xa > xb || ya > yb) continue;
+            int sidx = atomicAdd(&S.nsamp, 1);
+            if (sidx >= kFastSamples) {
+                S.overflow = 1;
+                break;
+            }
+            S.spos[sidx] = make_float2(px, py);
+            S.skey[sidx] = ((unsigned long long)pidx << 13) | (unsigned)k;
+            S.sslot[sidx] = (unsigned short)u;
+            for (int y = ya; y <= yb; y++) {
+                float wy = __fmaf_rn(-fabsf((float)y - py), invrad, 1.0f);
+                if (wy <= 0) continue;
+                for (int x = xa; x <= xb; x++) {
+                    float wx = __fmaf_rn(-fabsf((float)x - px), invrad, 1.0f);
+                    if (wx <= 0) continue;
+                    int q = (y - y0) * kT + (x - x0);
+                    int slot = atomicAdd(&S.tcnt[q], 1);
+                    if (slot < kTexelSlots)
+                        S.ent[q * kTexelSlots + slot] = (unsigned short)sidx;
+                    else
+                        S.overflow = 1;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (S.overflow) {
+        if (threadIdx.x == 0) slow_tiles[atomicAdd(slow_count, 1u)] = (unsigned)tile;
+        return;  // tile untouched; the sorted path redoes it
+    }
+    // per texel: order by (particle, k), then blend (upstream src/render.c:135-151)
+    float4 *face = reinterpret_cast<float4 *>(buf) + (size_t)f * R * R;
+    for (int q = threadIdx.x; q < kT * kT; q += kTB) {
+        const int lx = q % kT, ly = q / kT;
+        const int m = S.tcnt[q];
+        if (lx >= tw || ly >= th || (m == 0 && !C.renorm)) continue;
+        float4 *dp = face + (size_t)(y0 + ly) * R + x0 + lx;
+        float4 d = *dp;
+        if (C.renorm) {
+            d.x *= C.scale;
+            d.y *= C.scale;
+            d.z *= C.scale;
+            d.w *= C.scale;
+        }
+        unsigned short *e = S.ent + q * kTexelSlots;
+        for (int u = 1; u < m; u++) {
+            unsigned short key = e[u];
+            unsigned long long kk = S.skey[key];
+            int v = u - 1;
+            while (v >= 0 && S.skey[e[v]] > kk) {
+                e[v + 1] = e[v];
+                v--;
+            }
+            e[v + 1] = key;
+        }
+        const float xf = (float)(x0 + lx), yf = (float)(y0 + ly);
+        for (int u = 0; u < m; u++) {
+            int sdx = e[u];
+            float2 pp = S.spos[sdx];
+            float4 c = S.col[S.sslot[sdx]];
+            float w0 = C.alpha * c.w;
+            float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
+            float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
+            float w = __fmul_rn(__fmul_rn(w0, wx), wy);
+            float keep = 1.0f - w, add = __fmul_rn(w, invg);
+            d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
+            d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
+            d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
+            d.w = __fmaf_rn(d.w, keep, add);
+        }
+        *dp = d;
+    }
+}
+
 // Buffer renormalisation on its own (a second renormalisation falling due
 // before the next deposit).
 __global__ void k_scale(size_t n, float s, float *buf) {
@@ -497,8 +685,12 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
         k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->list);
         GGB_LAUNCHED();
     }
+    GGB_CHECK(cudaMemsetAsync(Pv->slow_count, 0, sizeof(unsigned), s));
+    k_rd_tiles_fast<<<Pv->ntiles, kTB, sizeof(FastSmem), s>>>(C, P->prev, P->pos, P->col, Pv->tile_start, Pv->list,
+                                                               r->buf, Pv->slow_tiles, Pv->slow_count);
+    GGB_LAUNCHED();
     k_rd_tiles<<<Pv->ntiles, kTB, sizeof(TileSmem), s>>>(C, P->prev, P->pos, P->col, Pv->tile_start, Pv->list,
-                                                           r->buf);
+                                                           r->buf, Pv->slow_tiles, Pv->slow_count);
     GGB_LAUNCHED();
     stage_end(ST_TILES);
     Pv->pending = false;
@@ -550,8 +742,11 @@ GGB_EXPORT int render_init(Render *r, int R, float radius, float alpha) {
     Pv->tile_count = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_start = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_fill = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
+    Pv->slow_tiles = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
+    Pv->slow_count = (unsigned *)dev_alloc(sizeof(unsigned));
     GGB_CHECK(cudaMallocHost(&Pv->total_host, sizeof(unsigned)));
     GGB_CHECK(cudaFuncSetAttribute(k_rd_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
+    GGB_CHECK(cudaFuncSetAttribute(k_rd_tiles_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FastSmem)));
     r->tr = reinterpret_cast<ThreadRecs *>(Pv);
     sync();
     return 0;
@@ -564,6 +759,8 @@ GGB_EXPORT void render_free(Render *r) {
         dev_free(Pv->tile_count);
         dev_free(Pv->tile_start);
         dev_free(Pv->tile_fill);
+        dev_free(Pv->slow_tiles);
+        dev_free(Pv->slow_count);
         dev_free(Pv->list);
         cudaFreeHost(Pv->total_host);
         if (Pv->mirror) cudaFreeHost(Pv->mirror);
@@ -657,4 +854,16 @@ GGB_EXPORT void ggb_render_read(const Render *r, float *out) {
     float g = (float)r->g;
     float sc = Pv->pending ? Pv->pending_scale : 1.f;
     for (size_t i = 0; i < n; i++) out[i] = Pv->pending ? (Pv->mirror[i] * sc) * g : Pv->mirror[i] * g;
+}
+
+// Diagnostics: tiles of the last deposit (all tiles, and those that took the
+// sorted fallback path) and the number of (particle, tile) list entries.
+GGB_EXPORT void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, unsigned *entries) {
+    RenderPriv *Pv = rpriv(r);
+    sync();
+    unsigned sc = 0;
+    GGB_CHECK(cudaMemcpy(&sc, Pv->slow_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (ntiles) *ntiles = (unsigned)Pv->ntiles;
+    if (slow_tiles) *slow_tiles = sc;
+    if (entries) *entries = *Pv->total_host;
 }

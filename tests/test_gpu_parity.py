@@ -240,6 +240,24 @@ def test_deposit_dense_tile_sorts_in_global_memory(gpu, orc32):
     assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
 
 
+def test_deposit_sample_overflow_takes_sorted_path(gpu, orc32):
+    """A tile whose particles are few (<= 1024) but whose samples overflow the
+    fast path's buffers (long arcs concentrated on one tile)."""
+    rng = np.random.default_rng(12)
+    n = 500
+    c = np.array([0.0, 0.0, 1.0])
+    prev = c + 0.03 * rng.normal(size=(n, 3))
+    prev /= np.linalg.norm(prev, axis=1, keepdims=True)
+    d = rng.normal(size=(n, 3))
+    d -= prev * np.sum(d * prev, 1, keepdims=True)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pos = prev * np.cos(0.1) + d * np.sin(0.1)
+    col = rng.uniform(0.1, 1, size=(n, 4))
+    a = K.deposit(gpu, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    b = K.deposit(orc32, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
+
+
 def test_fade_renormalisation(gpu, orc32):
     """g falls below 1e-4 (the buffer is rescaled, fused into the next deposit)."""
     prev, pos, col = K.random_arcs(500, seed=5, max_angle=0.05)
