@@ -60,6 +60,20 @@ void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, u
 void ggb_cell_of_batch(const CubeSphere *cs, const double *dirs, int n, int *out);
 void ggb_taps_batch(const CubeSphere *cs, const double *dirs, int n, int *idx, double *wt);
 
+/* No counterpart in the upstream code.  fluid_remove_mean without any device
+ * allocation, for callers that cannot allocate: processes whose device memory
+ * is entirely reserved up front by another allocator, and steady-state loops
+ * that must not call cudaMalloc / cudaFree (both synchronise the device).
+ * Removes the area-weighted mean of f[ncells] in place; f must already be
+ * device or managed memory.  Its scratch is one fixed 32 KB device array per
+ * GPU (held until the process exits), which limits grids to 16,777,216 cells
+ * (N <= 1672); larger grids, host buffers or a failed set-up return -1 with a
+ * message and leave f unchanged, success returns 0.  The first call on a
+ * device looks up the array's device address (once per device); make that
+ * first call before any stream capture.  All calls share the array, so calls
+ * whose GPU work overlaps (from several host threads) race. */
+int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f);
+
 /* Initial-condition parameters of the application driver (bands and curl noise). */
 typedef struct {
 	int bands;
