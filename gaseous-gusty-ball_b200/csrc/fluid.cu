@@ -17,6 +17,9 @@ int pcg_grid_size();
 int pcg_max_blocks();
 int pcg_block_size();
 void pcg_launch(const SolveParams &prm, cudaStream_t s);
+int pcg_check_structured(const LevelDev &F, const LevelDev &C);
+float *pcg_build_rw16(const LevelDev &F, const LevelDev &C);
+double *pcg_dense_map(const SolveParams &prm, int l0);
 
 constexpr int kB = 256;
 
@@ -264,6 +267,10 @@ struct FluidPriv {
     SolveResult *res_host = nullptr;
     unsigned int *vmax_bits = nullptr;
     unsigned int *vmax_host = nullptr;
+    int structured[kMaxLev] = {};  // level l -> l+1 transfers follow the index pattern
+    float *rw16[kMaxLev] = {};     // coarse-major structured restriction weights
+    double *dense = nullptr;       // dense map of the V-cycle below the grid levels
+    int nd = 0;
 };
 
 static FluidPriv *priv_of(const Fluid *F) {
@@ -277,6 +284,7 @@ static StencilDev stencil_of(const GridTables *t) {
     s.n = t->n;
     s.nring = t->nring;
     s.wslot = t->wslot;
+    s.wslot_d = t->wslot_d;
     s.ring_nb = t->ring_nb;
     s.ring_w = t->ring_w;
     return s;
@@ -334,9 +342,10 @@ static void build_levels(Fluid *F, FluidPriv *Pv) {
     }
 }
 
-constexpr int kBlockLevelMax = 1536;  // levels up to N=16 run inside one block (shared memory)
+constexpr int kBlockLevelMax = 1536;  // levels up to N=16 form the dense coarse map
 
 static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
+    if (F->cs->N > 3000) fail_msg("grids with N > 3000 exceed the solve kernel's staged window");
     SolveParams P;
     memset(&P, 0, sizeof(P));
     const bool mg = F->prm.multigrid != 0;
@@ -361,6 +370,8 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
             L.rstart = Pv->rstart[l];
             L.ridx = Pv->ridx[l];
             L.rw = Pv->rw[l];
+            L.structured = Pv->structured[l];
+            L.rw16 = Pv->rw16[l];
         }
     }
     if (mg && Pv->nlev >= 2) {
@@ -385,7 +396,30 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
     P.part = Pv->part;
     P.bar = Pv->bar;
     P.res = Pv->res;
+    if (mg && Pv->dense) {
+        P.dense = Pv->dense;
+        P.nd = Pv->nd;
+    }
     return P;
+}
+
+// Structured-transfer flags and the dense coarse map (after build_levels).
+static void finish_levels(Fluid *F, FluidPriv *Pv) {
+    SolveParams P = solve_params(F, Pv, 0, 1);
+    for (int l = 0; l + 1 < Pv->nlev; l++) {
+        LevelDev Fl = P.L[l], C = P.L[l + 1];
+        Fl.structured = 0;
+        Pv->structured[l] = pcg_check_structured(Fl, C);
+        if (Pv->structured[l]) Pv->rw16[l] = pcg_build_rw16(Fl, C);
+    }
+    if (Pv->nlev >= 2) {
+        P = solve_params(F, Pv, 0, 1);  // with the structured flags
+        int G = P.nlev_grid;
+        if (G < Pv->nlev && P.L[G].S.n <= kBlockLevelMax) {
+            Pv->dense = pcg_dense_map(P, G);
+            Pv->nd = P.L[G].S.n;
+        }
+    }
 }
 
 void solve_trace_target(unsigned long long **buf, int *cap);
@@ -485,6 +519,7 @@ GGB_EXPORT int fluid_init(Fluid *F, const CubeSphere *cs, const FluidParams *prm
     F->lev = Pv->lev;
     if (prm->multigrid) {
         build_levels(F, Pv);
+        finish_levels(F, Pv);
     } else {
         Pv->nlev = 0;
         Pv->lx[0] = (float *)dev_alloc(sizeof(float) * n);
@@ -521,6 +556,7 @@ GGB_EXPORT void fluid_free(Fluid *F) {
         dev_free(Pv->rstart[l]);
         dev_free(Pv->ridx[l]);
         dev_free(Pv->rw[l]);
+        dev_free(Pv->rw16[l]);
         dev_free(Pv->lx[l]);
         dev_free(Pv->lxo[l]);
         dev_free(Pv->lb[l]);
@@ -533,6 +569,7 @@ GGB_EXPORT void fluid_free(Fluid *F) {
     dev_free(Pv->bar);
     dev_free(Pv->res);
     dev_free(Pv->vmax_bits);
+    dev_free(Pv->dense);
     cudaFreeHost(Pv->res_host);
     cudaFreeHost(Pv->vmax_host);
     delete Pv;

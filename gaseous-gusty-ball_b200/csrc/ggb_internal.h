@@ -78,6 +78,7 @@ struct GridTables {
     // device-only
     int *ghost = nullptr;
     float *wslot = nullptr;
+    double *wslot_d = nullptr;  // the same four slot weights in FP64 (staged solver phases)
     int *ring_nb = nullptr;
     float *ring_w = nullptr;
     float *dinv = nullptr;

@@ -21,6 +21,8 @@ struct LevelDev {
     const int *rstart;  // [n_coarse+1] rows of R = P^T
     const int *ridx;    // fine cells of each row (ascending)
     const float *rw;    // weights of each row
+    int structured;     // 1: interior rows of R / P follow the 4x4 / 2x2 index pattern (verified at setup)
+    const float *rw16;  // [16][n_coarse] weights of the structured R rows (coarse-major), or nullptr
 };
 
 struct SolveResult {
@@ -49,6 +51,9 @@ struct SolveParams {
     int trace_cap;
     GridBarrier *bar;
     SolveResult *res;
+    // dense form of the V-cycle below the grid levels: xo_G = D b_G
+    const double *dense;  // [nd][nd] row-major, or nullptr
+    int nd;               // cells of level nlev_grid
 };
 
 }  // namespace ggb

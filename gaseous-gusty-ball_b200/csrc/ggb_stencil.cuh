@@ -11,6 +11,7 @@ namespace ggb {
 struct StencilDev {
     int N, n, nring;
     const float *wslot;   // [4][n]: E, N, NE, NW weights (0 = no link)
+    const double *wslot_d;  // the same in FP64
     const int *ring_nb;   // [6*nring][8], -1 terminated
     const float *ring_w;  // [6*nring][8]
 };
@@ -30,6 +31,29 @@ __device__ __forceinline__ void cell_fij(int c, int N, int &f, int &i, int &j) {
     int rem = c - f * nn;
     j = rem / N;
     i = rem - j * N;
+}
+
+// The links of a boundary-ring cell that leave the face: all eight (neighbour,
+// weight) pairs are loaded with two vector loads each, then every present
+// neighbour value is requested at once (two dependent rounds in total instead
+// of one per link).
+template <class X>
+__device__ __forceinline__ double ring_extras(const StencilDev &S, int f, int i, int j, double xc, X X_) {
+    const int r = ring_slot(f, i, j, S.N, S.nring);
+    const int4 *rn4 = reinterpret_cast<const int4 *>(S.ring_nb + r * kMaxNb);
+    const float4 *rw4 = reinterpret_cast<const float4 *>(S.ring_w + r * kMaxNb);
+    const int4 n0 = __ldg(rn4), n1 = __ldg(rn4 + 1);
+    const float4 q0 = __ldg(rw4), q1 = __ldg(rw4 + 1);
+    const int o[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};
+    const float q[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = o[k] >= 0 ? X_(o[k]) : xc;
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (o[k] >= 0) s += (double)q[k] * (xc - v[k]);
+    return s;
 }
 
 // sum over the links of cell c of w * (xc - X(nb)), accumulated in double.
@@ -70,15 +94,79 @@ __device__ __forceinline__ double apply_k(const StencilDev &S, int c, double xc,
     if (dn && (q = __ldg(ws + n + c - N)) != 0.f) s += (double)q * (xc - X_(c - N));
     if (w && dn && (q = __ldg(ws + 2 * n + c - N - 1)) != 0.f) s += (double)q * (xc - X_(c - N - 1));
     if (e && dn && (q = __ldg(ws + 3 * n + c - N + 1)) != 0.f) s += (double)q * (xc - X_(c - N + 1));
-    int r = ring_slot(f, i, j, N, S.nring);
-    const int *rn = S.ring_nb + r * kMaxNb;
-    const float *rw = S.ring_w + r * kMaxNb;
-    for (int k = 0; k < kMaxNb; k++) {
-        int o = __ldg(rn + k);
-        if (o < 0) break;
-        s += (double)__ldg(rw + k) * (xc - X_(o));
+    return s + ring_extras(S, f, i, j, xc, X_);
+}
+
+// K at cell c with the FP64 slot weights.  Neighbour values come from a block's
+// staged window x[k] (k in the window; every on-face neighbour of a cell of
+// the block's range lies in it) or, for links that leave the face, from
+// val(k) computed directly.  No FP32/FP64 conversions in the interior path.
+template <class Val>
+__device__ __forceinline__ double apply_k_staged(const StencilDev &S, int c, double xc, const double *x, Val val) {
+    const int N = S.N, n = S.n;
+    int f, i, j;
+    cell_fij(c, N, f, i, j);
+    const double *wd = S.wslot_d;
+    if (i > 0 && j > 0 && i + 1 < N && j + 1 < N) {
+        const double w0 = __ldg(wd + c), w1 = __ldg(wd + n + c), w2 = __ldg(wd + 2 * n + c),
+                     w3 = __ldg(wd + 3 * n + c), w4 = __ldg(wd + c - 1), w5 = __ldg(wd + n + c - N),
+                     w6 = __ldg(wd + 2 * n + c - N - 1), w7 = __ldg(wd + 3 * n + c - N + 1);
+        double s = w0 * (xc - x[c + 1]);
+        s += w1 * (xc - x[c + N]);
+        s += w2 * (xc - x[c + N + 1]);
+        s += w3 * (xc - x[c + N - 1]);
+        s += w4 * (xc - x[c - 1]);
+        s += w5 * (xc - x[c - N]);
+        s += w6 * (xc - x[c - N - 1]);
+        s += w7 * (xc - x[c - N + 1]);
+        return s;
     }
-    return s;
+    const bool e = i + 1 < N, w = i > 0, up = j + 1 < N, dn = j > 0;
+    double s = 0, q;
+    if (e && (q = __ldg(wd + c)) != 0.0) s += q * (xc - x[c + 1]);
+    if (up && (q = __ldg(wd + n + c)) != 0.0) s += q * (xc - x[c + N]);
+    if (e && up && (q = __ldg(wd + 2 * n + c)) != 0.0) s += q * (xc - x[c + N + 1]);
+    if (w && up && (q = __ldg(wd + 3 * n + c)) != 0.0) s += q * (xc - x[c + N - 1]);
+    if (w && (q = __ldg(wd + c - 1)) != 0.0) s += q * (xc - x[c - 1]);
+    if (dn && (q = __ldg(wd + n + c - N)) != 0.0) s += q * (xc - x[c - N]);
+    if (w && dn && (q = __ldg(wd + 2 * n + c - N - 1)) != 0.0) s += q * (xc - x[c - N - 1]);
+    if (e && dn && (q = __ldg(wd + 3 * n + c - N + 1)) != 0.0) s += q * (xc - x[c - N + 1]);
+    return s + ring_extras(S, f, i, j, xc, val);
+}
+
+// K at cell c with the window's values x[k] and FP64 slot weights w0..w3[k]
+// all staged in shared memory (indexed by cell; every on-face neighbour of a
+// cell of the block's range, and every slot weight the cell needs, lies in
+// the window).  Links that leave the face read val(k) and the ring tables.
+template <class Val>
+__device__ __forceinline__ double apply_k_smem(const StencilDev &S, int c, double xc, const double *x,
+                                               const double *wE, const double *wN, const double *wNE,
+                                               const double *wNW, Val val) {
+    const int N = S.N;
+    int f, i, j;
+    cell_fij(c, N, f, i, j);
+    if (i > 0 && j > 0 && i + 1 < N && j + 1 < N) {
+        double s = wE[c] * (xc - x[c + 1]);
+        s += wN[c] * (xc - x[c + N]);
+        s += wNE[c] * (xc - x[c + N + 1]);
+        s += wNW[c] * (xc - x[c + N - 1]);
+        s += wE[c - 1] * (xc - x[c - 1]);
+        s += wN[c - N] * (xc - x[c - N]);
+        s += wNE[c - N - 1] * (xc - x[c - N - 1]);
+        s += wNW[c - N + 1] * (xc - x[c - N + 1]);
+        return s;
+    }
+    const bool e = i + 1 < N, w = i > 0, up = j + 1 < N, dn = j > 0;
+    double s = 0, q;
+    if (e && (q = wE[c]) != 0.0) s += q * (xc - x[c + 1]);
+    if (up && (q = wN[c]) != 0.0) s += q * (xc - x[c + N]);
+    if (e && up && (q = wNE[c]) != 0.0) s += q * (xc - x[c + N + 1]);
+    if (w && up && (q = wNW[c]) != 0.0) s += q * (xc - x[c + N - 1]);
+    if (w && (q = wE[c - 1]) != 0.0) s += q * (xc - x[c - 1]);
+    if (dn && (q = wN[c - N]) != 0.0) s += q * (xc - x[c - N]);
+    if (w && dn && (q = wNE[c - N - 1]) != 0.0) s += q * (xc - x[c - N - 1]);
+    if (e && dn && (q = wNW[c - N + 1]) != 0.0) s += q * (xc - x[c - N + 1]);
+    return s + ring_extras(S, f, i, j, xc, val);
 }
 
 // The links of cell c as up to 8 (neighbour, weight) pairs; unused pairs have

@@ -337,6 +337,11 @@ __global__ void k_slots(int N, const unsigned char *nnb, const int *nbr, const f
     }
 }
 
+__global__ void k_to_double(size_t n, const float *src, double *dst) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 __global__ void k_sum_area(int n, const double *a, double *out) {
     // one block, fixed order
     __shared__ double s_red[kBlk / 32 + 2];
@@ -379,6 +384,7 @@ int grid_build(GridTables *t, int N, bool managed) {
     t->gc = (float *)talloc(managed, sizeof(float) * 3 * kMaxNb * n);
     t->ghost = (int *)dev_alloc(sizeof(int) * 6 * (4 * N + 4));
     t->wslot = (float *)dev_alloc(sizeof(float) * 4 * n);
+    t->wslot_d = (double *)dev_alloc(sizeof(double) * 4 * n);
     t->ring_nb = (int *)dev_alloc(sizeof(int) * kMaxNb * 6 * t->nring);
     t->ring_w = (float *)dev_alloc(sizeof(float) * kMaxNb * 6 * t->nring);
     t->dinv = (float *)dev_alloc(sizeof(float) * n);
@@ -400,6 +406,8 @@ int grid_build(GridTables *t, int N, bool managed) {
     k_weights<<<gb, kBlk, 0, s>>>(N, t->pos, t->nnb, t->nbr, symlen, t->w, t->elen, t->gc, t->dinv);
     GGB_LAUNCHED();
     k_slots<<<gb, kBlk, 0, s>>>(N, t->nnb, t->nbr, t->w, t->wslot, t->ring_nb, t->ring_w, counters + 2);
+    GGB_LAUNCHED();
+    k_to_double<<<gb, kBlk, 0, s>>>((size_t)4 * n, t->wslot, t->wslot_d);
     GGB_LAUNCHED();
     k_sum_area<<<1, kBlk, 0, s>>>(n, area64, tot);
     GGB_LAUNCHED();
@@ -435,6 +443,7 @@ void grid_release(GridTables *t) {
     tfree(m, t->gc);
     dev_free(t->ghost);
     dev_free(t->wslot);
+    dev_free(t->wslot_d);
     dev_free(t->ring_nb);
     dev_free(t->ring_w);
     dev_free(t->dinv);

@@ -6,22 +6,32 @@
 //
 // Upstream: src/fluid.c:41-160 (multigrid), :264-275 (mean), :290-358 (PCG).
 // The arithmetic of every vector update follows upstream (FP32 vectors, FP64
-// accumulation); the schedule is this library's: phases are separated by a
-// bounded grid-wide barrier instead of host loops, the neighbour values of a
-// freshly updated vector are recomputed on the fly where that saves a
-// barrier (p = z + beta p inside K p; r - alpha Ap inside the level-0
-// pre-smooth), and the small coarse levels run inside thread block 0.
+// accumulation); the schedule is this library's:
+//   * phases are separated by a bounded grid-wide barrier instead of host loops;
+//   * each block owns a contiguous range of cells of every level; a stencil
+//     phase first computes the (transformed) neighbour value of every cell of
+//     the range plus its halo once, in FP64, into shared memory, then applies
+//     the stencil with FP64 weights (no FP32/FP64 conversion per link);
+//   * p = z + beta p and r - alpha Ap are recomputed inside K p and the level-0
+//     pre-smooth, which saves two barriers per iteration;
+//   * interior rows of R and P use index arithmetic (no CSR indirection);
+//   * the V-cycle below the grid levels (N <= 16, at most 1536 cells) is a
+//     fixed linear map, precomputed once as a dense matrix and applied by all
+//     blocks from L2.
 #include <algorithm>
 #include <cstdio>
+#include <vector>
 
 #include "ggb_internal.h"
 #include "ggb_solver.h"
 
 namespace ggb {
 
-constexpr int kPB = 512;           // threads per block of the persistent kernel
-constexpr double kOmegaJ = 0.8;    // upstream MG_OMEGA
-constexpr double kCorrScale = 1.0; // upstream MG_CORR_SCALE
+constexpr int kPB = 512;            // threads per block of the persistent kernel
+constexpr double kOmegaJ = 0.8;     // upstream MG_OMEGA
+constexpr double kCorrScale = 1.0;  // upstream MG_CORR_SCALE
+constexpr int kStageCap = 3584;     // cells of a block's staged window (value + 4 slot weights FP64, 3 FP32 own inputs)
+constexpr size_t kStageBytes = (size_t)kStageCap * (5 * sizeof(double) + 3 * sizeof(float));
 
 enum { RED_BB = 0, RED_RR, RED_PAP, RED_RZ, RED_MEAN, RED_AREA, RED_N };
 
@@ -40,60 +50,10 @@ __device__ __forceinline__ void trace_mark(const SolveParams &P, int mark) {
 
 #define GRID_LOOP(c, n) for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < (n); c += gridDim.x * blockDim.x)
 #define BLOCK_LOOP(c, n) for (int c = threadIdx.x; c < (n); c += blockDim.x)
-
-// ---- per-cell pieces of the V-cycle -------------------------------------
-
-// Pre-smooth from x = 0 with right-hand side b: x = w D^-1 b, r = b - K x
-// (x at the neighbours recomputed from b).
-template <class B>
-__device__ __forceinline__ void presmooth_cell(const LevelDev &L, int c, B bval) {
-    const float *dv = L.dinv;
-    auto X = [&](int k) -> double { return (double)(float)(kOmegaJ * __ldg(dv + k) * bval(k)); };
-    float bc = bval(c);
-    float xc = (float)(kOmegaJ * __ldg(dv + c) * bc);
-    double kx = apply_k(L.S, c, (double)xc, X);
-    L.x[c] = xc;
-    L.r[c] = (float)(bc - kx);
-}
-
-// b_coarse[c] = sum over row c of R of rw * r_fine.
-__device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev &C, int c) {
-    int k0 = __ldg(F.rstart + c), k1 = __ldg(F.rstart + c + 1);
-    double acc = 0;
-    int k = k0;
-    for (; k + 4 <= k1; k += 4) {  // four independent gathers per round
-        int i0 = __ldg(F.ridx + k), i1 = __ldg(F.ridx + k + 1), i2 = __ldg(F.ridx + k + 2), i3 = __ldg(F.ridx + k + 3);
-        float w0 = __ldg(F.rw + k), w1 = __ldg(F.rw + k + 1), w2 = __ldg(F.rw + k + 2), w3 = __ldg(F.rw + k + 3);
-        float r0 = F.r[i0], r1 = F.r[i1], r2 = F.r[i2], r3 = F.r[i3];
-        acc += (double)(w0 * r0);
-        acc += (double)(w1 * r1);
-        acc += (double)(w2 * r2);
-        acc += (double)(w3 * r3);
-    }
-    for (; k < k1; k++) acc += (double)(__ldg(F.rw + k) * F.r[__ldg(F.ridx + k)]);
-    C.b[c] = (float)acc;
-}
-
-// x_fine += P xo_coarse.
-__device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &C, int i) {
-    const int *t = F.ptap + 4 * i;
-    const float *w = F.pw + 4 * i;
-    const float *xc = C.xo;
-    float s = __ldg(w) * xc[__ldg(t)] + __ldg(w + 1) * xc[__ldg(t + 1)] + __ldg(w + 2) * xc[__ldg(t + 2)] +
-              __ldg(w + 3) * xc[__ldg(t + 3)];
-    F.x[i] += (float)(kCorrScale * s);
-}
-
-// One damped-Jacobi sweep src -> dst: dst = src + w D^-1 (b - K src).
-__device__ __forceinline__ float jacobi_cell(const StencilDev &S, const float *dinv, const float *b, const float *src,
-                                             float *dst, int c) {
-    auto X = [&](int k) -> double { return (double)src[k]; };
-    float xc = src[c];
-    float rc = (float)(b[c] - apply_k(S, c, (double)xc, X));
-    float out = xc + (float)(kOmegaJ * __ldg(dinv + c) * rc);
-    dst[c] = out;
-    return out;
-}
+#define SYNC_OR(fail)                    \
+    do {                                 \
+        if (!grid_sync(P.bar)) fail;     \
+    } while (0)
 
 struct Red {
     double v[kPB / 32 + 2];
@@ -107,10 +67,192 @@ __device__ __forceinline__ double get_total(const SolveParams &P, int which, dou
     return sum_partials<kPB>(P.part + which * gridDim.x, gridDim.x, s_red);
 }
 
-// ---- the coarse levels inside block 0, vectors in shared memory ----------
-// Levels l0..nlev-1 have at most kBlockCells cells in total; each gets x, xo,
-// b, r slices of the dynamic shared memory.  The operator tables stay in
-// global memory (read-only, L1-cached).
+// ---- staged stencil phases ------------------------------------------------
+
+__device__ __forceinline__ void block_range(int n, int &c0, int &c1) {
+    c0 = (int)(((long long)n * blockIdx.x) / gridDim.x);
+    c1 = (int)(((long long)n * (blockIdx.x + 1)) / gridDim.x);
+}
+
+// cell(c, x, wE, wN, wNE, wNW) for every cell c of this block's range of a
+// level; over the stencil window of the current sub-range, x[k] = val(k) and
+// the four slot weights are staged (FP64) in shared memory, all with
+// independent loads issued together.  Ends with a block barrier.
+__device__ unsigned long long *g_stage_trace;  // diagnostics: block 0 stamps staging / compute ends
+__device__ int g_stage_trace_n;
+__device__ __forceinline__ void stage_mark(int mark) {
+    unsigned long long *t = g_stage_trace;
+    if (t && blockIdx.x == 0 && threadIdx.x == 0) {
+        int k = g_stage_trace_n;
+        if (k < 4096) {
+            t[2 * k] = (unsigned long long)mark;
+            t[2 * k + 1] = globaltimer_ns();
+            g_stage_trace_n = k + 1;
+        }
+    }
+}
+
+struct Own {
+    float a, b, c;
+};
+
+// cell(c, x, wE, wN, wNE, wNW, o) for every cell c of this block's range of a
+// level.  Over the stencil window of the current sub-range, x[k] = val(k) and
+// the four slot weights are staged (FP64) in shared memory, and own(k) (up to
+// three FP32 inputs of the cell itself) for the cells of the sub-range; all
+// global loads happen in the staging loop, where they are independent, so the
+// compute loop reads shared memory only.  Ends with a block barrier.
+template <class Val, class OwnF, class Cell>
+__device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val, OwnF own, Cell cell) {
+    const int N = S.N, n = S.n;
+    int c0, c1;
+    block_range(n, c0, c1);
+    const int halo = N + 1;
+    const int sub = kStageCap - 2 * halo;
+    double *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap,
+           *b3 = buf + 4 * kStageCap;
+    float *oa = reinterpret_cast<float *>(buf + 5 * kStageCap), *ob = oa + kStageCap, *oc = ob + kStageCap;
+    const double *wd = S.wslot_d;
+    stage_mark(1);
+    for (int s0 = c0; s0 < c1; s0 += sub) {
+        const int s1 = min(c1, s0 + sub);
+        const int w0 = max(0, s0 - halo), w1 = min(n, s1 + halo);
+        for (int k = w0 + threadIdx.x; k < w1; k += blockDim.x) {
+            const int q = k - w0;
+            const double e = __ldg(wd + k), nn = __ldg(wd + n + k), ne = __ldg(wd + 2 * n + k),
+                         nw = __ldg(wd + 3 * n + k);
+            bx[q] = val(k);
+            b0[q] = e;
+            b1[q] = nn;
+            b2[q] = ne;
+            b3[q] = nw;
+            if (k >= s0 && k < s1) {
+                Own o = own(k);
+                oa[k - s0] = o.a;
+                ob[k - s0] = o.b;
+                oc[k - s0] = o.c;
+            }
+        }
+        __syncthreads();
+        stage_mark(2);
+        for (int c = s0 + threadIdx.x; c < s1; c += blockDim.x) {
+            Own o;
+            o.a = oa[c - s0];
+            o.b = ob[c - s0];
+            o.c = oc[c - s0];
+            cell(c, bx - w0, b0 - w0, b1 - w0, b2 - w0, b3 - w0, o);
+        }
+        __syncthreads();
+        stage_mark(3);
+    }
+}
+
+#define STAGED_ARGS const double *x, const double *wE, const double *wN, const double *wNE, const double *wNW, Own o
+#define APPLY(S, c, xc) apply_k_smem(S, c, xc, x, wE, wN, wNE, wNW, val)
+
+// The pre-smoothed iterate from 0 at cell k: w D^-1 b.
+__device__ __forceinline__ float presmooth_x(const LevelDev &L, int k, float b) {
+    return (float)(kOmegaJ * __ldg(L.dinv + k) * b);
+}
+
+// Pre-smooth of a level from x = 0 with right-hand side b: x = w D^-1 b,
+// r = b - K x.
+__device__ __forceinline__ void phase_presmooth(const LevelDev &L, const float *b, double *buf) {
+    auto val = [&](int k) -> double { return (double)presmooth_x(L, k, b[k]); };
+    auto own = [&](int k) -> Own { return Own{b[k], 0.f, 0.f}; };
+    staged(L.S, buf, val, own, [&](int c, STAGED_ARGS) {
+        const float bc = o.a;
+        const float xc = (float)x[c];  // = presmooth_x(L, c, bc)
+        const double kx = APPLY(L.S, c, (double)xc);
+        L.x[c] = xc;
+        L.r[c] = (float)(bc - kx);
+    });
+}
+
+// Post-smooth: xo = x + w D^-1 (b - K x); returns sum dotr . xo when dotr != nullptr.
+__device__ __forceinline__ double phase_postsmooth(const LevelDev &L, const float *b, float *xo, const float *dotr,
+                                                   double *buf) {
+    double s = 0;
+    const float *xs = L.x;
+    auto val = [&](int k) -> double { return (double)xs[k]; };
+    auto own = [&](int k) -> Own { return Own{b[k], __ldg(L.dinv + k), dotr ? dotr[k] : 0.f}; };
+    staged(L.S, buf, val, own, [&](int c, STAGED_ARGS) {
+        const float xc = (float)x[c];
+        const float rc = (float)(o.a - APPLY(L.S, c, (double)xc));
+        const float out = xc + (float)(kOmegaJ * o.b * rc);
+        xo[c] = out;
+        s += (double)o.c * out;
+    });
+    return s;
+}
+
+// b_coarse = R r_fine.  Interior coarse cells gather their 4x4 fine window in
+// the CSR row order (fine index ascending) with the P weights; the others use
+// the CSR rows.
+__device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev &C, int c) {
+    const int Nc = C.S.N, Nf = F.S.N;
+    int f, I, J;
+    cell_fij(c, Nc, f, I, J);
+    double acc = 0;
+    if (F.structured && I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc) {
+        const float *r = F.r;
+        const int base = (f * Nf + 2 * J - 1) * Nf + 2 * I - 1;
+        const int nc = C.S.n;
+        float wv[16], rv[16];
+#pragma unroll
+        for (int dj = 0; dj < 4; dj++)
+#pragma unroll
+            for (int di = 0; di < 4; di++) {
+                const int i = base + dj * Nf + di;
+                wv[dj * 4 + di] = __ldg(F.rw16 + (dj * 4 + di) * nc + c);
+                rv[dj * 4 + di] = r[i];
+            }
+#pragma unroll
+        for (int q = 0; q < 16; q++) acc += (double)(wv[q] * rv[q]);
+    } else {
+        const int k0 = __ldg(F.rstart + c), k1 = __ldg(F.rstart + c + 1);
+        for (int k = k0; k < k1; k++) acc += (double)(__ldg(F.rw + k) * F.r[__ldg(F.ridx + k)]);
+    }
+    C.b[c] = (float)acc;
+}
+
+// x_fine += P xo_coarse.  Interior fine cells compute their 2x2 coarse taps.
+__device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &C, int i) {
+    const int Nf = F.S.N, Nc = C.S.N;
+    const float4 w = __ldg(reinterpret_cast<const float4 *>(F.pw) + i);
+    const float *xc = C.xo;
+    int t0, t1, t2, t3;
+    int f, fi, fj;
+    cell_fij(i, Nf, f, fi, fj);
+    const int I0 = (fi - 1) >> 1, J0 = (fj - 1) >> 1;
+    if (F.structured && I0 >= 0 && J0 >= 0 && I0 + 1 < Nc && J0 + 1 < Nc) {
+        t0 = (f * Nc + J0) * Nc + I0;
+        t1 = t0 + 1;
+        t2 = t0 + Nc;
+        t3 = t0 + Nc + 1;
+    } else {
+        const int4 t = __ldg(reinterpret_cast<const int4 *>(F.ptap) + i);
+        t0 = t.x;
+        t1 = t.y;
+        t2 = t.z;
+        t3 = t.w;
+    }
+    const float s = w.x * xc[t0] + w.y * xc[t1] + w.z * xc[t2] + w.w * xc[t3];
+    F.x[i] += (float)(kCorrScale * s);
+}
+
+// One damped-Jacobi sweep src -> dst with per-link conversions (small levels).
+__device__ __forceinline__ float jacobi_cell(const StencilDev &S, const float *dinv, const float *b, const float *src,
+                                             float *dst, int c) {
+    auto X = [&](int k) -> double { return (double)src[k]; };
+    float xc = src[c];
+    float rc = (float)(b[c] - apply_k(S, c, (double)xc, X));
+    float out = xc + (float)(kOmegaJ * __ldg(dinv + c) * rc);
+    dst[c] = out;
+    return out;
+}
+
+// ---- the coarse levels inside one block (setup of the dense map, fallback) --
 
 struct SmemLevel {
     float *x, *xo, *b, *r;
@@ -129,8 +271,7 @@ __device__ void carve_smem(const SolveParams &P, int l0, float *smem, SmemLevel 
 }
 
 // Coarsest level: `sweeps` Jacobi sweeps from 0; result in V.xo.  When every
-// cell has its own thread, the cell's links, 1/diag and b stay in registers
-// for all sweeps (the level has ~100 cells and 60 sweeps are latency-bound).
+// cell has its own thread, the cell's links, 1/diag and b stay in registers.
 __device__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps) {
     const int n = L.S.n;
     BLOCK_LOOP(c, n) V.x[c] = 0.f;
@@ -175,30 +316,31 @@ __device__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps)
     }
 }
 
-// Levels l0..nlev-1 of the V-cycle inside this block.  Reads b of level l0
-// from global memory and writes xo of level l0 back to global memory.
-__device__ void vcycle_block(const SolveParams &P, int l0, float *smem) {
-    SmemLevel lv[kMaxLev];
-    carve_smem(P, l0, smem, lv);
+// Levels l0..nlev-1 of the V-cycle inside this block, on vectors in shared
+// memory.  b of level l0 is lv[l0].b on entry; xo of level l0 is written to
+// `out` (global memory).
+__device__ void vcycle_block_smem(const SolveParams &P, int l0, SmemLevel *lv, float *out) {
     const int last = P.nlev - 1;
-    BLOCK_LOOP(c, P.L[l0].S.n) lv[l0].b[c] = P.L[l0].b[c];
-    __syncthreads();
     for (int l = l0; l < last; l++) {
         LevelDev L = P.L[l];
         L.x = lv[l].x;
         L.r = lv[l].r;
         const float *b = lv[l].b;
-        BLOCK_LOOP(c, L.S.n) presmooth_cell(L, c, [&](int k) -> float { return b[k]; });
+        BLOCK_LOOP(c, L.S.n) {
+            auto X = [&](int k) -> double { return (double)(float)(kOmegaJ * __ldg(L.dinv + k) * b[k]); };
+            float bc = b[c];
+            float xc = (float)(kOmegaJ * __ldg(L.dinv + c) * bc);
+            double kx = apply_k(L.S, c, (double)xc, X);
+            L.x[c] = xc;
+            L.r[c] = (float)(bc - kx);
+        }
         __syncthreads();
-        trace_mark(P, 2000 + l);
         LevelDev C = P.L[l + 1];
         C.b = lv[l + 1].b;
         BLOCK_LOOP(c, C.S.n) restrict_cell(L, C, c);
         __syncthreads();
-        trace_mark(P, 2100 + l);
     }
     coarsest_smem(P.L[last], lv[last], P.coarse_sweeps);
-    trace_mark(P, 2200);
     for (int l = last - 1; l >= l0; l--) {
         LevelDev L = P.L[l];
         L.x = lv[l].x;
@@ -206,81 +348,89 @@ __device__ void vcycle_block(const SolveParams &P, int l0, float *smem) {
         C.xo = lv[l + 1].xo;
         BLOCK_LOOP(i, L.S.n) prolong_cell(L, C, i);
         __syncthreads();
-        trace_mark(P, 2300 + l);
-        float *xo = l == l0 ? P.L[l0].xo : lv[l].xo;  // level l0's result goes to global memory
-        BLOCK_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, lv[l].b, lv[l].x, xo, c);
-        __syncthreads();
-        trace_mark(P, 2400 + l);
-    }
-    if (l0 == last) {
-        BLOCK_LOOP(c, P.L[last].S.n) P.L[last].xo[c] = lv[last].xo[c];
+        BLOCK_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, lv[l].b, lv[l].x, lv[l].xo, c);
         __syncthreads();
     }
+    BLOCK_LOOP(c, P.L[l0].S.n) out[c] = lv[l0].xo[c];
+    __syncthreads();
 }
+
+// ---- the V-cycle after level 0's pre-smooth --------------------------------
 
 // The rest of z = V(r) once level 0's pre-smooth (x, r of level 0) is complete
 // and visible.  Ends with rz = r . z published; returns false on abort.
-__device__ bool vcycle_rest(const SolveParams &P, const float *r, double *s_red, float *smem) {
+__device__ bool vcycle_rest(const SolveParams &P, const float *r, double *s_red, double *buf, float *smem) {
     const int G = P.nlev_grid;
-    const int last = P.nlev - 1;
-    // down: restrict level 0, then pre-smooth + restrict the other grid levels
+    // down
     for (int l = 0; l < G; l++) {
         const LevelDev &L = P.L[l];
         if (l > 0) {
-            GRID_LOOP(c, L.S.n) presmooth_cell(L, c, [&](int k) -> float { return L.b[k]; });
+            phase_presmooth(L, L.b, buf);
             trace_mark(P, 100 + l);
-            if (!grid_sync(P.bar)) return false;
-            trace_mark(P, 200 + l);
+            SYNC_OR(return false);
         }
         GRID_LOOP(c, P.L[l + 1].S.n) restrict_cell(L, P.L[l + 1], c);
         trace_mark(P, 300 + l);
-        if (!grid_sync(P.bar)) return false;
-        trace_mark(P, 400 + l);
+        SYNC_OR(return false);
     }
-    // the coarse part
-    if (!P.coarse_on_grid) {
-        if (blockIdx.x == 0) vcycle_block(P, G, smem);
+    // below the grid levels: the dense map, or block 0
+    if (P.dense) {
+        const LevelDev &C = P.L[G];
+        const int nd = P.nd, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+        for (int row = gw; row < nd; row += nw) {
+            const double *d = P.dense + (size_t)row * nd;
+            double acc = 0;
+            for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)C.b[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) C.xo[row] = (float)acc;
+        }
         trace_mark(P, 500);
-        if (!grid_sync(P.bar)) return false;
-        trace_mark(P, 600);
+        SYNC_OR(return false);
+    } else if (!P.coarse_on_grid) {
+        if (blockIdx.x == 0) {
+            SmemLevel lv[kMaxLev];
+            carve_smem(P, G, smem, lv);
+            BLOCK_LOOP(c, P.L[G].S.n) lv[G].b[c] = P.L[G].b[c];
+            __syncthreads();
+            vcycle_block_smem(P, G, lv, P.L[G].xo);
+        }
+        trace_mark(P, 500);
+        SYNC_OR(return false);
     } else {
-        // G == last: the coarsest level is large, sweep it grid-wide
-        const LevelDev &L = P.L[last];
+        // the coarsest level is large (nlev_grid == nlev - 1): sweep it grid-wide
+        const LevelDev &L = P.L[P.nlev - 1];
         GRID_LOOP(c, L.S.n) L.x[c] = 0.f;
-        if (!grid_sync(P.bar)) return false;
+        SYNC_OR(return false);
         float *src = L.x, *dst = L.xo;
         for (int s = 0; s < P.coarse_sweeps; s++) {
             GRID_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, L.b, src, dst, c);
-            if (!grid_sync(P.bar)) return false;
+            SYNC_OR(return false);
             float *t = src;
             src = dst;
             dst = t;
         }
         if (src != L.xo) {
             GRID_LOOP(c, L.S.n) L.xo[c] = src[c];
-            if (!grid_sync(P.bar)) return false;
+            SYNC_OR(return false);
         }
     }
-    // up: prolong + post-smooth; level 0 writes z and the rz partial
+    // up
     for (int l = G - 1; l >= 0; l--) {
         const LevelDev &L = P.L[l];
         GRID_LOOP(i, L.S.n) prolong_cell(L, P.L[l + 1], i);
         trace_mark(P, 700 + l);
-        if (!grid_sync(P.bar)) return false;
-        trace_mark(P, 800 + l);
+        SYNC_OR(return false);
         if (l > 0) {
-            GRID_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, L.b, L.x, L.xo, c);
+            phase_postsmooth(L, L.b, L.xo, nullptr, buf);
             trace_mark(P, 900 + l);
-            if (!grid_sync(P.bar)) return false;
-            trace_mark(P, 1000 + l);
+            SYNC_OR(return false);
         } else {
-            double s = 0;
-            GRID_LOOP(c, L.S.n) {
-                float z = jacobi_cell(L.S, L.dinv, r, L.x, P.z, c);
-                s += (double)r[c] * z;
-            }
+            double s = phase_postsmooth(L, r, P.z, r, buf);
             put_partial(P, RED_RZ, s, s_red);
-            if (!grid_sync(P.bar)) return false;
+            trace_mark(P, 900);
+            SYNC_OR(return false);
         }
     }
     return true;
@@ -300,11 +450,11 @@ __device__ bool single_level(const SolveParams &P, const float *r, double *s_red
         }
     } else {
         GRID_LOOP(c, L.S.n) L.x[c] = 0.f;
-        if (!grid_sync(P.bar)) return false;
+        SYNC_OR(return false);
         float *src = L.x, *dst = L.xo;
         for (int s = 0; s < P.coarse_sweeps; s++) {
             GRID_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, r, src, dst, c);
-            if (!grid_sync(P.bar)) return false;
+            SYNC_OR(return false);
             float *t = src;
             src = dst;
             dst = t;
@@ -313,7 +463,7 @@ __device__ bool single_level(const SolveParams &P, const float *r, double *s_red
             GRID_LOOP(c, L.S.n) L.xo[c] = src[c];
         }
     }
-    if (!grid_sync(P.bar)) return false;
+    SYNC_OR(return false);
     double s = 0;
     GRID_LOOP(c, L.S.n) {
         float z = L.xo[c];
@@ -326,7 +476,9 @@ __device__ bool single_level(const SolveParams &P, const float *r, double *s_red
 
 __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     __shared__ Red sh;
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) unsigned char dyn[];
+    double *buf = reinterpret_cast<double *>(dyn);               // staged window
+    float *smem = reinterpret_cast<float *>(dyn + kStageBytes);  // block-0 levels
     double *s_red = sh.v;
     const LevelDev &L0 = P.L[0];
     const StencilDev &S0 = L0.S;
@@ -334,7 +486,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     const bool mg = P.nlev >= 2;
     const bool single = P.nlev == 1;
     float *r = P.r, *rn = P.r2, *p = P.p, *pn = P.p2;
-    double bb, rr, rz = 0, tol2, beta = 0;
+    double bb, rr, rz = 0, tol2, beta = 0, m2;
     int it = 0;
     bool first = true, ok = true;
 
@@ -343,7 +495,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         double s = 0;
         GRID_LOOP(c, n) s += (double)__ldg(P.area + c) * P.omega[c];
         put_partial(P, RED_MEAN, s, s_red);
-        if (!grid_sync(P.bar)) goto aborted;
+        SYNC_OR(goto aborted);
         float m = (float)(get_total(P, RED_MEAN, s_red) / P.total_area);
         GRID_LOOP(c, n) P.omega[c] -= m;  // read back below only at the own cell
     }
@@ -354,7 +506,6 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     // sum b = 0 to double precision.  Without it the constant mode of the
     // residual stays at the FP32 rounding level and CG diverges once the
     // residual reaches it.
-    double m2;
     {
         double s = 0, sa = 0;
         GRID_LOOP(c, n) {
@@ -364,7 +515,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         }
         put_partial(P, RED_MEAN, s, s_red);
         put_partial(P, RED_AREA, sa, s_red);
-        if (!grid_sync(P.bar)) goto aborted;
+        SYNC_OR(goto aborted);
         m2 = get_total(P, RED_MEAN, s_red) / get_total(P, RED_AREA, s_red);
     }
 
@@ -372,18 +523,19 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     {
         double sb = 0, sr = 0;
         const float *psi = P.psi;
-        auto X = [&](int k) -> double { return (double)psi[k]; };
-        GRID_LOOP(c, n) {
-            double b = -(double)__ldg(P.area + c) * ((double)P.omega[c] - m2);
-            double ri = b - apply_k(S0, c, (double)psi[c], X);
+        auto val = [&](int k) -> double { return (double)psi[k]; };
+        auto own = [&](int k) -> Own { return Own{P.omega[k], __ldg(P.area + k), 0.f}; };
+        staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+            double b = -(double)o.b * ((double)o.a - m2);
+            double ri = b - APPLY(S0, c, x[c]);
             r[c] = (float)ri;
             sb += b * b;
             sr += ri * ri;
-        }
+        });
         put_partial(P, RED_BB, sb, s_red);
         put_partial(P, RED_RR, sr, s_red);
     }
-    if (!grid_sync(P.bar)) goto aborted;
+    SYNC_OR(goto aborted);
     bb = get_total(P, RED_BB, s_red);
     rr = get_total(P, RED_RR, s_red);
     if (bb == 0.0) {
@@ -401,9 +553,9 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     // z = M^-1 r, rz
     if (rr > tol2) {
         if (mg) {
-            GRID_LOOP(c, n) presmooth_cell(L0, c, [&](int k) -> float { return r[k]; });
-            if (!grid_sync(P.bar)) goto aborted;
-            ok = vcycle_rest(P, r, s_red, smem);
+            phase_presmooth(L0, r, buf);
+            SYNC_OR(goto aborted);
+            ok = vcycle_rest(P, r, s_red, buf, smem);
         } else if (single) {
             ok = single_level(P, r, s_red, smem);
         } else {
@@ -427,16 +579,18 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             const float *po = p;
             const bool fst = first;
             const double be = beta;
-            auto PN = [&](int k) -> float { return fst ? z[k] : (float)(z[k] + be * po[k]); };
-            auto X = [&](int k) -> double { return (double)PN(k); };
+            auto pnew = [&](int k) -> float { return fst ? z[k] : (float)(z[k] + be * po[k]); };
+            auto val = [&](int k) -> double { return (double)pnew(k); };
+            auto own = [&](int) -> Own { return Own{0.f, 0.f, 0.f}; };
             double s = 0;
-            GRID_LOOP(c, n) {
-                float pc = PN(c);
-                double a = apply_k(S0, c, (double)pc, X);
-                pn[c] = pc;
-                P.Ap[c] = (float)a;
+            float *pw = pn, *ap = P.Ap;
+            staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+                const float pc = (float)x[c];
+                const double a = APPLY(S0, c, (double)pc);
+                pw[c] = pc;
+                ap[c] = (float)a;
                 s += a * pc;
-            }
+            });
             put_partial(P, RED_PAP, s, s_red);
             float *t = p;
             p = pn;
@@ -444,7 +598,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             first = false;
         }
         trace_mark(P, 10);
-        if (!grid_sync(P.bar)) goto aborted;
+        SYNC_OR(goto aborted);
         trace_mark(P, 11);
         {
             double pAp = get_total(P, RED_PAP, s_red);
@@ -452,23 +606,34 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             const double alpha = rz / pAp;
             const float *Ap = P.Ap;
             const float *ro = r;
+            const float *pp = p;
             double s = 0, sz = 0;
+            float *rw_ = rn;
             if (mg) {
                 // psi += alpha p; r' = r - alpha Ap; level-0 pre-smooth of r'
-                auto RN = [&](int k) -> float { return (float)(ro[k] - alpha * Ap[k]); };
-                GRID_LOOP(c, n) {
-                    P.psi[c] += (float)(alpha * p[c]);
-                    double ri = ro[c] - alpha * Ap[c];
-                    rn[c] = (float)ri;
+                auto rnew = [&](int k) -> float { return (float)(ro[k] - alpha * Ap[k]); };
+                auto val = [&](int k) -> double { return (double)presmooth_x(L0, k, rnew(k)); };
+                // own: r, Ap of the cell; psi += alpha p happens here too (nothing else reads psi)
+                auto own = [&](int k) -> Own {
+                    P.psi[k] += (float)(alpha * pp[k]);
+                    return Own{ro[k], Ap[k], 0.f};
+                };
+                staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+                    const double ri = o.a - alpha * o.b;
+                    const float rc = (float)ri;
+                    rw_[c] = rc;
                     s += ri * ri;
-                    presmooth_cell(L0, c, RN);
-                }
+                    const float xc = (float)x[c];  // = presmooth_x(L0, c, rc)
+                    const double kx = APPLY(S0, c, (double)xc);
+                    L0.x[c] = xc;
+                    L0.r[c] = (float)(rc - kx);
+                });
             } else {
                 GRID_LOOP(c, n) {
-                    P.psi[c] += (float)(alpha * p[c]);
+                    P.psi[c] += (float)(alpha * pp[c]);
                     double ri = ro[c] - alpha * Ap[c];
                     float rc = (float)ri;
-                    rn[c] = rc;
+                    rw_[c] = rc;
                     s += ri * ri;
                     if (!single) {
                         float z = __ldg(L0.dinv + c) * rc;
@@ -485,12 +650,12 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         }
         it++;
         trace_mark(P, 12);
-        if (!grid_sync(P.bar)) goto aborted;
+        SYNC_OR(goto aborted);
         trace_mark(P, 13);
         rr = get_total(P, RED_RR, s_red);
         if (rr <= tol2) break;
         if (mg)
-            ok = vcycle_rest(P, r, s_red, smem);
+            ok = vcycle_rest(P, r, s_red, buf, smem);
         else if (single)
             ok = single_level(P, r, s_red, smem);
         if (!ok) goto aborted;
@@ -502,13 +667,13 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     }
 
     // zero-mean projection of psi
-    if (!grid_sync(P.bar)) goto aborted;
+    SYNC_OR(goto aborted);
     {
         double s = 0;
         GRID_LOOP(c, n) s += (double)__ldg(P.area + c) * P.psi[c];
         put_partial(P, RED_MEAN, s, s_red);
     }
-    if (!grid_sync(P.bar)) goto aborted;
+    SYNC_OR(goto aborted);
     {
         float m = (float)(get_total(P, RED_MEAN, s_red) / P.total_area);
         GRID_LOOP(c, n) P.psi[c] -= m;
@@ -532,6 +697,73 @@ aborted:
     }
 }
 
+// ---- setup kernels -------------------------------------------------------
+
+// Column j of the dense map of levels l0..nlev-1: the block's V-cycle applied
+// to the unit vector e_j, stored row-major D[row][j] in FP64.
+__global__ void __launch_bounds__(kPB, 1) k_dense_columns(SolveParams P, int l0, float *colbuf, double *D) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    float *smem = reinterpret_cast<float *>(dyn);
+    const int nd = P.L[l0].S.n;
+    for (int j = blockIdx.x; j < nd; j += gridDim.x) {
+        SmemLevel lv[kMaxLev];
+        carve_smem(P, l0, smem, lv);
+        BLOCK_LOOP(c, nd) lv[l0].b[c] = c == j ? 1.0f : 0.0f;
+        __syncthreads();
+        float *col = colbuf + (size_t)blockIdx.x * nd;
+        vcycle_block_smem(P, l0, lv, col);
+        BLOCK_LOOP(c, nd) D[(size_t)c * nd + j] = col[c];
+        __syncthreads();
+    }
+}
+
+// Coarse-major weights of the structured rows of R: rw16[q][c] = the weight of
+// fine cell q (q = 4*dj + di of the 4x4 window) in row c, taken from the CSR
+// row (which the structured check has verified to be that window in order).
+__global__ void k_build_rw16(LevelDev F, LevelDev C, float *rw16) {
+    const int Nc = C.S.N, nc = C.S.n;
+    GRID_LOOP(c, nc) {
+        int f, I, J;
+        cell_fij(c, Nc, f, I, J);
+        const bool inner = I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc;
+        const int k0 = F.rstart[c];
+        for (int q = 0; q < 16; q++) rw16[q * nc + c] = inner ? F.rw[k0 + q] : 0.f;
+    }
+}
+
+// Counts rows of R / taps of P of a level pair that the structured path would
+// take but that do not follow the structured index pattern.
+__global__ void k_check_structured(LevelDev F, LevelDev C, int *bad) {
+    const int Nf = F.S.N, Nc = C.S.N;
+    GRID_LOOP(c, C.S.n) {
+        int f, I, J;
+        cell_fij(c, Nc, f, I, J);
+        if (!(I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc)) continue;
+        int k0 = F.rstart[c], k1 = F.rstart[c + 1];
+        if (k1 - k0 != 16) {
+            atomicAdd(bad, 1);
+            continue;
+        }
+        const int base = (f * Nf + 2 * J - 1) * Nf + 2 * I - 1;
+        for (int dj = 0; dj < 4; dj++)
+            for (int di = 0; di < 4; di++) {
+                const int i = base + dj * Nf + di, q = k0 + dj * 4 + di;
+                const int k = (di <= 1 ? 1 : 0) + 2 * (dj <= 1 ? 1 : 0);
+                if (F.ridx[q] != i || F.rw[q] != F.pw[4 * i + k]) atomicAdd(bad, 1);
+            }
+    }
+    GRID_LOOP(i, F.S.n) {
+        int f, fi, fj;
+        cell_fij(i, Nf, f, fi, fj);
+        const int I0 = (fi - 1) >> 1, J0 = (fj - 1) >> 1;
+        if (!(I0 >= 0 && J0 >= 0 && I0 + 1 < Nc && J0 + 1 < Nc)) continue;
+        const int t0 = (f * Nc + J0) * Nc + I0;
+        if (F.ptap[4 * i] != t0 || F.ptap[4 * i + 1] != t0 + 1 || F.ptap[4 * i + 2] != t0 + Nc ||
+            F.ptap[4 * i + 3] != t0 + Nc + 1)
+            atomicAdd(bad, 1);
+    }
+}
+
 // ---------------------------------------------------------------- host
 
 int pcg_block_size() { return kPB; }
@@ -543,30 +775,36 @@ void solve_trace_target(unsigned long long **buf, int *cap) {
     *cap = g_trace_cap;
 }
 
-// Dynamic shared memory of a launch: x, xo, b, r of every level run by block 0.
+// Dynamic shared memory of a launch: the staged window, plus x, xo, b, r of
+// every level run by block 0.
 static size_t pcg_smem_bytes(const SolveParams &p) {
     size_t cells = 0;
-    if (p.nlev >= 2 && !p.coarse_on_grid)
+    if (p.nlev >= 2 && !p.dense && !p.coarse_on_grid)
         for (int l = p.nlev_grid; l < p.nlev; l++) cells += p.L[l].S.n;
     if (p.nlev == 1 && !p.coarse_on_grid) cells = p.L[0].S.n;
-    return 4 * sizeof(float) * cells;
+    return kStageBytes + 4 * sizeof(float) * cells;
 }
 
 int pcg_max_blocks() { return 2 * device_sm_count(); }
 
-static int pcg_grid_for(size_t smem) {
+static void pcg_attributes() {
     static bool attr = false;
     if (!attr) {
-        GGB_CHECK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        GGB_CHECK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        GGB_CHECK(cudaFuncSetAttribute(k_dense_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
+}
+
+static int pcg_grid_for(size_t smem) {
+    pcg_attributes();
     int per = 0;
     GGB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg, kPB, smem));
     if (per < 1) fail_msg("the solve kernel cannot be resident on this device (%zu B shared memory)", smem);
     return device_sm_count() * std::min(per, 2);
 }
 
-int pcg_grid_size() { return pcg_grid_for(0); }
+int pcg_grid_size() { return pcg_grid_for(kStageBytes); }
 
 void pcg_launch(const SolveParams &prm, cudaStream_t s) {
     SolveParams p = prm;
@@ -574,6 +812,44 @@ void pcg_launch(const SolveParams &prm, cudaStream_t s) {
     void *args[] = {&p};
     GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(pcg_grid_for(smem)), dim3(kPB), args, smem, s));
     GGB_LAUNCHED();
+}
+
+// Coarse-major structured restriction weights of a level pair (after the check).
+float *pcg_build_rw16(const LevelDev &F, const LevelDev &C) {
+    float *rw16 = (float *)dev_alloc(sizeof(float) * 16 * (size_t)C.S.n);
+    k_build_rw16<<<std::max(1u, std::min(grid_for(C.S.n, 256), 2048u)), 256, 0, stream()>>>(F, C, rw16);
+    GGB_LAUNCHED();
+    return rw16;
+}
+
+// Verifies the structured index pattern of a level pair's R / P (1 = usable).
+int pcg_check_structured(const LevelDev &F, const LevelDev &C) {
+    int *bad = (int *)dev_alloc(sizeof(int));
+    k_check_structured<<<std::max(1u, std::min(grid_for(F.S.n, 256), 2048u)), 256, 0, stream()>>>(F, C, bad);
+    GGB_LAUNCHED();
+    int hb = 0;
+    GGB_CHECK(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+    GGB_CHECK(cudaStreamSynchronize(stream()));
+    dev_free(bad);
+    return hb == 0;
+}
+
+// The dense map of the V-cycle of levels l0..nlev-1 (nd x nd, FP64).
+double *pcg_dense_map(const SolveParams &prm, int l0) {
+    SolveParams p = prm;
+    const int nd = p.L[l0].S.n;
+    size_t cells = 0;
+    for (int l = l0; l < p.nlev; l++) cells += p.L[l].S.n;
+    size_t smem = 4 * sizeof(float) * cells;
+    pcg_attributes();
+    int grid = std::min(nd, 4 * device_sm_count());
+    double *D = (double *)dev_alloc(sizeof(double) * nd * nd);
+    float *colbuf = (float *)dev_alloc(sizeof(float) * (size_t)grid * nd);
+    k_dense_columns<<<grid, kPB, smem, stream()>>>(p, l0, colbuf, D);
+    GGB_LAUNCHED();
+    GGB_CHECK(cudaStreamSynchronize(stream()));
+    dev_free(colbuf);
+    return D;
 }
 
 // ---- micro-benchmark of the grid barrier (additive entry point) ----------
@@ -639,4 +915,23 @@ GGB_EXPORT int ggb_solve_trace(unsigned long long *out, int cap) {
     n = n < cap ? n : cap;
     if (n > 0) GGB_CHECK(cudaMemcpy(out, g_trace_dev, sizeof(unsigned long long) * 2 * n, cudaMemcpyDeviceToHost));
     return n;
+}
+
+GGB_EXPORT int ggb_stage_trace(int enable, unsigned long long *out, int cap) {
+    using namespace ggb;
+    sync();
+    static unsigned long long *buf = nullptr;
+    int n = 0;
+    if (!enable) {
+        GGB_CHECK(cudaMemcpyFromSymbol(&n, g_stage_trace_n, sizeof(int)));
+        n = n < cap ? n : cap;
+        if (n > 0 && buf) GGB_CHECK(cudaMemcpy(out, buf, sizeof(unsigned long long) * 2 * n, cudaMemcpyDeviceToHost));
+        unsigned long long *null = nullptr;
+        GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace, &null, sizeof(null)));
+        return n;
+    }
+    if (!buf) buf = (unsigned long long *)dev_alloc(sizeof(unsigned long long) * 2 * 4096);
+    GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace, &buf, sizeof(buf)));
+    GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace_n, &n, sizeof(int)));
+    return 0;
 }
