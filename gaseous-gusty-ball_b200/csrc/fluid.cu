@@ -15,6 +15,7 @@ namespace ggb {
 
 int pcg_grid_size();
 int pcg_max_blocks();
+int pcg_max_grid_n();
 int pcg_block_size();
 void pcg_launch(const SolveParams &prm, cudaStream_t s);
 int pcg_check_structured(const LevelDev &F, const LevelDev &C);
@@ -345,7 +346,8 @@ static void build_levels(Fluid *F, FluidPriv *Pv) {
 constexpr int kBlockLevelMax = 1536;  // levels up to N=16 form the dense coarse map
 
 static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
-    if (F->cs->N > 3000) fail_msg("grids with N > 3000 exceed the solve kernel's staged window");
+    if (F->cs->N > pcg_max_grid_n())
+        fail_msg("grids with N > %d exceed the solve kernel's staged window (N = %d)", pcg_max_grid_n(), F->cs->N);
     SolveParams P;
     memset(&P, 0, sizeof(P));
     const bool mg = F->prm.multigrid != 0;

@@ -132,6 +132,13 @@ __device__ __forceinline__ int ghost_cell_direct(int f, int i, int j, int N, dou
     return cell_of(centre_dir(f, i, j, h), N, h);
 }
 
+// Position of boundary-ring cell (i, j) among its face's ring cells in cell
+// order: row 0, then the two end cells of every middle row, then row N-1.
+// For any cell it is the number of the face's ring cells before it.
+__host__ __device__ __forceinline__ int ring_rank_in_face(int i, int j, int N) {
+    return j == 0 ? i : (j < N - 1 ? N + 2 * (j - 1) + (i > 0) : 3 * N - 4 + i);
+}
+
 // Index of ghost (i, j), i, j in [-1, N], into a face's ring table of 4N+4 entries.
 __host__ __device__ __forceinline__ int ghost_ring_index(int i, int j, int N) {
     if (j == -1) return i + 1;

@@ -16,13 +16,11 @@ struct StencilDev {
     const float *ring_w;  // [6*nring][8]
 };
 
+// Row of the ring tables for boundary-ring cell (f, i, j): the tables are in
+// cell order (ring rank), so the ring cells of a cell range own one contiguous
+// block of rows.
 __device__ __forceinline__ int ring_slot(int f, int i, int j, int N, int nring) {
-    int r;
-    if (j == 0) r = i;
-    else if (j == N - 1) r = N + i;
-    else if (i == 0) r = 2 * N + (j - 1);
-    else r = 2 * N + (N - 2) + (j - 1);
-    return f * nring + r;
+    return f * nring + ring_rank_in_face(i, j, N);
 }
 
 __device__ __forceinline__ void cell_fij(int c, int N, int &f, int &i, int &j) {
@@ -97,76 +95,53 @@ __device__ __forceinline__ double apply_k(const StencilDev &S, int c, double xc,
     return s + ring_extras(S, f, i, j, xc, X_);
 }
 
-// K at cell c with the FP64 slot weights.  Neighbour values come from a block's
-// staged window x[k] (k in the window; every on-face neighbour of a cell of
-// the block's range lies in it) or, for links that leave the face, from
-// val(k) computed directly.  No FP32/FP64 conversions in the interior path.
-template <class Val>
-__device__ __forceinline__ double apply_k_staged(const StencilDev &S, int c, double xc, const double *x, Val val) {
-    const int N = S.N, n = S.n;
+// Boundary-ring cells in cell order: the number of ring cells with index
+// below c (c in [0, n]), and the cell of ring rank R.
+__device__ __forceinline__ int ring_rank_below(int c, int N, int nring) {
     int f, i, j;
     cell_fij(c, N, f, i, j);
-    const double *wd = S.wslot_d;
-    if (i > 0 && j > 0 && i + 1 < N && j + 1 < N) {
-        const double w0 = __ldg(wd + c), w1 = __ldg(wd + n + c), w2 = __ldg(wd + 2 * n + c),
-                     w3 = __ldg(wd + 3 * n + c), w4 = __ldg(wd + c - 1), w5 = __ldg(wd + n + c - N),
-                     w6 = __ldg(wd + 2 * n + c - N - 1), w7 = __ldg(wd + 3 * n + c - N + 1);
-        double s = w0 * (xc - x[c + 1]);
-        s += w1 * (xc - x[c + N]);
-        s += w2 * (xc - x[c + N + 1]);
-        s += w3 * (xc - x[c + N - 1]);
-        s += w4 * (xc - x[c - 1]);
-        s += w5 * (xc - x[c - N]);
-        s += w6 * (xc - x[c - N - 1]);
-        s += w7 * (xc - x[c - N + 1]);
-        return s;
+    return f * nring + ring_rank_in_face(i, j, N);
+}
+__device__ __forceinline__ void ring_cell_of_rank(int R, int N, int nring, int &f, int &i, int &j) {
+    f = R / nring;
+    const int q = R - f * nring;
+    if (q < N) {
+        j = 0;
+        i = q;
+    } else if (q < 3 * N - 4) {
+        const int m = q - N;
+        j = 1 + (m >> 1);
+        i = (m & 1) ? N - 1 : 0;
+    } else {
+        j = N - 1;
+        i = q - (3 * N - 4);
     }
-    const bool e = i + 1 < N, w = i > 0, up = j + 1 < N, dn = j > 0;
-    double s = 0, q;
-    if (e && (q = __ldg(wd + c)) != 0.0) s += q * (xc - x[c + 1]);
-    if (up && (q = __ldg(wd + n + c)) != 0.0) s += q * (xc - x[c + N]);
-    if (e && up && (q = __ldg(wd + 2 * n + c)) != 0.0) s += q * (xc - x[c + N + 1]);
-    if (w && up && (q = __ldg(wd + 3 * n + c)) != 0.0) s += q * (xc - x[c + N - 1]);
-    if (w && (q = __ldg(wd + c - 1)) != 0.0) s += q * (xc - x[c - 1]);
-    if (dn && (q = __ldg(wd + n + c - N)) != 0.0) s += q * (xc - x[c - N]);
-    if (w && dn && (q = __ldg(wd + 2 * n + c - N - 1)) != 0.0) s += q * (xc - x[c - N - 1]);
-    if (e && dn && (q = __ldg(wd + 3 * n + c - N + 1)) != 0.0) s += q * (xc - x[c - N + 1]);
-    return s + ring_extras(S, f, i, j, xc, val);
 }
 
 // K at cell c with the window's values x[k] and FP64 slot weights w0..w3[k]
-// all staged in shared memory (indexed by cell; every on-face neighbour of a
-// cell of the block's range, and every slot weight the cell needs, lies in
-// the window).  Links that leave the face read val(k) and the ring tables.
-template <class Val>
+// all staged in shared memory (indexed by cell; the window spans [c - N - 1,
+// c + N + 1] for every cell c of the block's range, zero-filled where it
+// runs past the ends of the grid).  One branch-free formula serves every
+// cell: a slot whose link would leave the face has weight 0 in the layout
+// (also where the neighbouring index wraps to another row or face), so its
+// term adds an exact zero.  A boundary-ring cell adds the staged sum of its
+// links that leave the face, rsum[ring rank - r0].
 __device__ __forceinline__ double apply_k_smem(const StencilDev &S, int c, double xc, const double *x,
                                                const double *wE, const double *wN, const double *wNE,
-                                               const double *wNW, Val val) {
+                                               const double *wNW, const double *rsum, int r0) {
     const int N = S.N;
     int f, i, j;
     cell_fij(c, N, f, i, j);
-    if (i > 0 && j > 0 && i + 1 < N && j + 1 < N) {
-        double s = wE[c] * (xc - x[c + 1]);
-        s += wN[c] * (xc - x[c + N]);
-        s += wNE[c] * (xc - x[c + N + 1]);
-        s += wNW[c] * (xc - x[c + N - 1]);
-        s += wE[c - 1] * (xc - x[c - 1]);
-        s += wN[c - N] * (xc - x[c - N]);
-        s += wNE[c - N - 1] * (xc - x[c - N - 1]);
-        s += wNW[c - N + 1] * (xc - x[c - N + 1]);
-        return s;
-    }
-    const bool e = i + 1 < N, w = i > 0, up = j + 1 < N, dn = j > 0;
-    double s = 0, q;
-    if (e && (q = wE[c]) != 0.0) s += q * (xc - x[c + 1]);
-    if (up && (q = wN[c]) != 0.0) s += q * (xc - x[c + N]);
-    if (e && up && (q = wNE[c]) != 0.0) s += q * (xc - x[c + N + 1]);
-    if (w && up && (q = wNW[c]) != 0.0) s += q * (xc - x[c + N - 1]);
-    if (w && (q = wE[c - 1]) != 0.0) s += q * (xc - x[c - 1]);
-    if (dn && (q = wN[c - N]) != 0.0) s += q * (xc - x[c - N]);
-    if (w && dn && (q = wNE[c - N - 1]) != 0.0) s += q * (xc - x[c - N - 1]);
-    if (e && dn && (q = wNW[c - N + 1]) != 0.0) s += q * (xc - x[c - N + 1]);
-    return s + ring_extras(S, f, i, j, xc, val);
+    double s = wE[c] * (xc - x[c + 1]);
+    s += wN[c] * (xc - x[c + N]);
+    s += wNE[c] * (xc - x[c + N + 1]);
+    s += wNW[c] * (xc - x[c + N - 1]);
+    s += wE[c - 1] * (xc - x[c - 1]);
+    s += wN[c - N] * (xc - x[c - N]);
+    s += wNE[c - N - 1] * (xc - x[c - N - 1]);
+    s += wNW[c - N + 1] * (xc - x[c - N + 1]);
+    if (i == 0 || j == 0 || i == N - 1 || j == N - 1) s += rsum[f * S.nring + ring_rank_in_face(i, j, N) - r0];
+    return s;
 }
 
 // The links of cell c as up to 8 (neighbour, weight) pairs; unused pairs have

@@ -281,13 +281,6 @@ __global__ void k_weights(int N, const float *pos, unsigned char *nnb, int *nbr,
     }
 }
 
-__host__ __device__ __forceinline__ int ring_index_of(int i, int j, int N) {
-    if (j == 0) return i;
-    if (j == N - 1) return N + i;
-    if (i == 0) return 2 * N + (j - 1);
-    return 2 * N + (N - 2) + (j - 1);
-}
-
 // Face-tiled layout: direction slots for on-face links inside the 3x3 box;
 // everything else of a ring cell goes to its ring list.  `bad` counts
 // interior cells with a link outside their 3x3 box (the layout requires 0)
@@ -299,7 +292,7 @@ __global__ void k_slots(int N, const unsigned char *nnb, const int *nbr, const f
         int f, i, j;
         decode(c, N, f, i, j);
         bool ring = i == 0 || j == 0 || i == N - 1 || j == N - 1;
-        int r = ring ? f * nring + ring_index_of(i, j, N) : -1;
+        int r = ring ? f * nring + ring_rank_in_face(i, j, N) : -1;
         int nx = 0;
         for (int k = 0; k < nnb[c]; k++) {
             int o = nbr[kMaxNb * c + k];
@@ -333,7 +326,10 @@ __global__ void k_slots(int N, const unsigned char *nnb, const int *nbr, const f
             }
         }
         if (ring)
-            for (int k = nx; k < kMaxNb; k++) ring_nb[r * kMaxNb + k] = -1;
+            for (int k = nx; k < kMaxNb; k++) {
+                ring_nb[r * kMaxNb + k] = -1;
+                ring_w[r * kMaxNb + k] = 0.f;
+            }
     }
 }
 

@@ -31,7 +31,9 @@ constexpr int kPB = 512;            // threads per block of the persistent kerne
 constexpr double kOmegaJ = 0.8;     // upstream MG_OMEGA
 constexpr double kCorrScale = 1.0;  // upstream MG_CORR_SCALE
 constexpr int kStageCap = 3584;     // cells of a block's staged window (value + 4 slot weights FP64, 3 FP32 own inputs)
-constexpr size_t kStageBytes = (size_t)kStageCap * (5 * sizeof(double) + 3 * sizeof(float));
+constexpr int kRingCap = 1024;      // boundary-ring cells of one staged sub-range (their off-face link sums)
+constexpr int kStageWords = kStageCap * 5 + (kStageCap * 3 + 1) / 2 + kRingCap;  // in doubles
+constexpr size_t kStageBytes = (size_t)kStageWords * sizeof(double);
 
 enum { RED_BB = 0, RED_RR, RED_PAP, RED_RZ, RED_MEAN, RED_AREA, RED_N };
 
@@ -80,9 +82,17 @@ __device__ __forceinline__ void block_range(int n, int &c0, int &c1) {
 // independent loads issued together.  Ends with a block barrier.
 __device__ unsigned long long *g_stage_trace;  // diagnostics: block 0 stamps staging / compute ends
 __device__ int g_stage_trace_n;
+__device__ int g_stage_trace_all;  // 1: every block records, mark | block << 16
 __device__ __forceinline__ void stage_mark(int mark) {
     unsigned long long *t = g_stage_trace;
-    if (t && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!t || threadIdx.x != 0) return;
+    if (g_stage_trace_all) {
+        const int k = atomicAdd(&g_stage_trace_n, 1);
+        if (k < 4096) {
+            t[2 * k] = (unsigned long long)(mark | (blockIdx.x << 16));
+            t[2 * k + 1] = globaltimer_ns();
+        }
+    } else if (blockIdx.x == 0) {
         int k = g_stage_trace_n;
         if (k < 4096) {
             t[2 * k] = (unsigned long long)mark;
@@ -96,15 +106,18 @@ struct Own {
     float a, b, c;
 };
 
-// cell(c, x, wE, wN, wNE, wNW, o) for every cell c of this block's range of a
-// level.  Over the stencil window of the current sub-range, x[k] = val(k) and
-// the four slot weights are staged (FP64) in shared memory, and own(k) (up to
-// three FP32 inputs of the cell itself) for the cells of the sub-range; all
-// global loads happen in the staging loop, where they are independent, so the
+// cell(c, x, wE, wN, wNE, wNW, rsum, r0, o) for every cell c of this block's
+// range of a level.  Over the stencil window of the current sub-range, x[k] =
+// val(k) and the four slot weights are staged (FP64) in shared memory, and
+// own(k) (up to three FP32 inputs of the cell itself) for the cells of the
+// sub-range.  The links that leave a face (boundary-ring cells) are summed in
+// the staging pass as well, one thread per link and a fixed-order 8-lane tree
+// per ring cell: rsum[ring rank - r0] = sum_k w_k (val(c) - val(nb_k)).  All
+// global loads happen while staging, where they are independent, so the
 // compute loop reads shared memory only.  Ends with a block barrier.
 template <class Val, class OwnF, class Cell>
 __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val, OwnF own, Cell cell) {
-    const int N = S.N, n = S.n;
+    const int N = S.N, n = S.n, nring = S.nring, bs = blockDim.x, tid = threadIdx.x;
     int c0, c1;
     block_range(n, c0, c1);
     const int halo = N + 1;
@@ -112,43 +125,145 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val
     double *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap,
            *b3 = buf + 4 * kStageCap;
     float *oa = reinterpret_cast<float *>(buf + 5 * kStageCap), *ob = oa + kStageCap, *oc = ob + kStageCap;
+    double *rs = buf + kStageWords - kRingCap;
     const double *wd = S.wslot_d;
     stage_mark(1);
-    for (int s0 = c0; s0 < c1; s0 += sub) {
-        const int s1 = min(c1, s0 + sub);
-        const int w0 = max(0, s0 - halo), w1 = min(n, s1 + halo);
-        for (int k = w0 + threadIdx.x; k < w1; k += blockDim.x) {
-            const int q = k - w0;
-            const double e = __ldg(wd + k), nn = __ldg(wd + n + k), ne = __ldg(wd + 2 * n + k),
-                         nw = __ldg(wd + 3 * n + k);
-            bx[q] = val(k);
-            b0[q] = e;
-            b1[q] = nn;
-            b2[q] = ne;
-            b3[q] = nw;
-            if (k >= s0 && k < s1) {
-                Own o = own(k);
-                oa[k - s0] = o.a;
-                ob[k - s0] = o.b;
-                oc[k - s0] = o.c;
+    for (int s0 = c0; s0 < c1;) {
+        int s1 = min(c1, s0 + sub);
+        const int r0 = ring_rank_below(s0, N, nring);
+        int r1 = ring_rank_below(s1, N, nring);
+        if (r1 - r0 > kRingCap) {  // end the sub-range before its (kRingCap+1)-th ring cell
+            r1 = r0 + kRingCap;
+            int f, i, j;
+            ring_cell_of_rank(r1, N, nring, f, i, j);
+            s1 = (f * N + j) * N + i;
+        }
+        const int w0 = s0 - halo, w1 = s1 + halo;  // cells outside [0, n) stage as zeros
+        // The ring tables are in ring-rank order: this sub-range's boundary-ring
+        // cells are rows r0..r1-1, one thread per ring cell.  The first row of
+        // each thread (its eight links as two 16-byte loads each) and its own
+        // value are fetched before the window loop so that their latency
+        // overlaps it.
+        const int nr = r1 - r0;
+        const int4 *rn4 = reinterpret_cast<const int4 *>(S.ring_nb) + 2 * (size_t)r0;
+        const float4 *rw4 = reinterpret_cast<const float4 *>(S.ring_w) + 2 * (size_t)r0;
+        int4 fo0 = make_int4(-1, -1, -1, -1), fo1 = fo0;
+        float4 fw0 = make_float4(0.f, 0.f, 0.f, 0.f), fw1 = fw0;
+        double fvc = 0;
+        if (tid < nr) {
+            fo0 = __ldg(rn4 + 2 * tid);
+            fo1 = __ldg(rn4 + 2 * tid + 1);
+            fw0 = __ldg(rw4 + 2 * tid);
+            fw1 = __ldg(rw4 + 2 * tid + 1);
+            int f, i, j;
+            ring_cell_of_rank(r0 + tid, N, nring, f, i, j);
+            fvc = val((f * N + j) * N + i);
+        }
+        // window: values and slot weights, two cells per thread per pass with
+        // every global load of both issued before any shared-memory store
+        for (int k = w0 + tid; k < w1; k += 2 * bs) {
+            const int k2 = k + bs;
+            const bool two = k2 < w1;
+            double e1 = 0, n1 = 0, ne1 = 0, nw1 = 0, v1 = 0;
+            if (k >= 0 && k < n) {
+                e1 = __ldg(wd + k);
+                n1 = __ldg(wd + n + k);
+                ne1 = __ldg(wd + 2 * n + k);
+                nw1 = __ldg(wd + 3 * n + k);
+                v1 = val(k);
             }
+            double e2 = 0, n2 = 0, ne2 = 0, nw2 = 0, v2 = 0;
+            if (two && k2 >= 0 && k2 < n) {
+                e2 = __ldg(wd + k2);
+                n2 = __ldg(wd + n + k2);
+                ne2 = __ldg(wd + 2 * n + k2);
+                nw2 = __ldg(wd + 3 * n + k2);
+                v2 = val(k2);
+            }
+            const bool in1 = k >= s0 && k < s1, in2 = two && k2 >= s0 && k2 < s1;
+            Own o1{0.f, 0.f, 0.f}, o2{0.f, 0.f, 0.f};
+            if (in1) o1 = own(k);
+            if (in2) o2 = own(k2);
+            int q = k - w0;
+            bx[q] = v1;
+            b0[q] = e1;
+            b1[q] = n1;
+            b2[q] = ne1;
+            b3[q] = nw1;
+            if (in1) {
+                oa[k - s0] = o1.a;
+                ob[k - s0] = o1.b;
+                oc[k - s0] = o1.c;
+            }
+            if (two) {
+                q = k2 - w0;
+                bx[q] = v2;
+                b0[q] = e2;
+                b1[q] = n2;
+                b2[q] = ne2;
+                b3[q] = nw2;
+            }
+            if (in2) {
+                oa[k2 - s0] = o2.a;
+                ob[k2 - s0] = o2.b;
+                oc[k2 - s0] = o2.c;
+            }
+        }
+        // off-face links of each ring cell: all present neighbour values
+        // requested at once, summed in link order
+        for (int q = tid; q < nr; q += bs) {
+            int4 o0, o1;
+            float4 w0v, w1v;
+            double vc;
+            if (q == tid) {
+                o0 = fo0;
+                o1 = fo1;
+                w0v = fw0;
+                w1v = fw1;
+                vc = fvc;
+            } else {
+                o0 = __ldg(rn4 + 2 * q);
+                o1 = __ldg(rn4 + 2 * q + 1);
+                w0v = __ldg(rw4 + 2 * q);
+                w1v = __ldg(rw4 + 2 * q + 1);
+                int f, i, j;
+                ring_cell_of_rank(r0 + q, N, nring, f, i, j);
+                vc = val((f * N + j) * N + i);
+            }
+            const int o[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
+            const float w[8] = {w0v.x, w0v.y, w0v.z, w0v.w, w1v.x, w1v.y, w1v.z, w1v.w};
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = o[k] >= 0 ? val(o[k]) : vc;
+            double t = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (o[k] >= 0) t += (double)w[k] * (vc - v[k]);
+            rs[q] = t;
         }
         __syncthreads();
         stage_mark(2);
-        for (int c = s0 + threadIdx.x; c < s1; c += blockDim.x) {
+        // two independent cells in flight per thread: one cell's dependent
+        // chain (shared loads, FP64 sum, conversions) leaves the issue slots
+        // idle with 16 warps per SM
+#pragma unroll 2
+        for (int c = s0 + tid; c < s1; c += bs) {
             Own o;
             o.a = oa[c - s0];
             o.b = ob[c - s0];
             o.c = oc[c - s0];
-            cell(c, bx - w0, b0 - w0, b1 - w0, b2 - w0, b3 - w0, o);
+            cell(c, bx - w0, b0 - w0, b1 - w0, b2 - w0, b3 - w0, rs, r0, o);
         }
         __syncthreads();
         stage_mark(3);
+        s0 = s1;
     }
 }
 
-#define STAGED_ARGS const double *x, const double *wE, const double *wN, const double *wNE, const double *wNW, Own o
-#define APPLY(S, c, xc) apply_k_smem(S, c, xc, x, wE, wN, wNE, wNW, val)
+#define STAGED_ARGS                                                                                             \
+    const double *x, const double *wE, const double *wN, const double *wNE, const double *wNW, const double *rsum, \
+        int r0, Own o
+#define APPLY(S, c, xc) apply_k_smem(S, c, xc, x, wE, wN, wNE, wNW, rsum, r0)
 
 // The pre-smoothed iterate from 0 at cell k: w D^-1 b.
 __device__ __forceinline__ float presmooth_x(const LevelDev &L, int k, float b) {
@@ -787,10 +902,20 @@ static size_t pcg_smem_bytes(const SolveParams &p) {
 
 int pcg_max_blocks() { return 2 * device_sm_count(); }
 
+// Largest level edge N whose staged window (a block's cells plus N + 1 on
+// either side) leaves at least one block of threads' worth of cells per pass.
+int pcg_max_grid_n() { return (kStageCap - kPB) / 2 - 1; }
+
 static void pcg_attributes() {
     static bool attr = false;
     if (!attr) {
-        GGB_CHECK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        int dev = 0, optin = 0;
+        GGB_CHECK(cudaGetDevice(&dev));
+        GGB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        GGB_CHECK(cudaFuncGetAttributes(&fa, k_pcg));
+        GGB_CHECK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin - (int)fa.sharedSizeBytes));
         GGB_CHECK(cudaFuncSetAttribute(k_dense_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
@@ -917,6 +1042,10 @@ GGB_EXPORT int ggb_solve_trace(unsigned long long *out, int cap) {
     return n;
 }
 
+// Diagnostics: enable = 1 makes block 0 of the next solves stamp the start,
+// staged and computed points of every staged phase (mark, ns); enable = 2 makes
+// every block stamp them (mark | block << 16, ns); enable = 0 stops and copies
+// out up to cap records, returning their number.
 GGB_EXPORT int ggb_stage_trace(int enable, unsigned long long *out, int cap) {
     using namespace ggb;
     sync();
@@ -925,6 +1054,7 @@ GGB_EXPORT int ggb_stage_trace(int enable, unsigned long long *out, int cap) {
     if (!enable) {
         GGB_CHECK(cudaMemcpyFromSymbol(&n, g_stage_trace_n, sizeof(int)));
         n = n < cap ? n : cap;
+        n = n < 4096 ? n : 4096;
         if (n > 0 && buf) GGB_CHECK(cudaMemcpy(out, buf, sizeof(unsigned long long) * 2 * n, cudaMemcpyDeviceToHost));
         unsigned long long *null = nullptr;
         GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace, &null, sizeof(null)));
@@ -933,5 +1063,7 @@ GGB_EXPORT int ggb_stage_trace(int enable, unsigned long long *out, int cap) {
     if (!buf) buf = (unsigned long long *)dev_alloc(sizeof(unsigned long long) * 2 * 4096);
     GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace, &buf, sizeof(buf)));
     GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace_n, &n, sizeof(int)));
+    const int all = enable == 2;
+    GGB_CHECK(cudaMemcpyToSymbol(g_stage_trace_all, &all, sizeof(int)));
     return 0;
 }
