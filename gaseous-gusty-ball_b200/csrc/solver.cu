@@ -76,10 +76,6 @@ __device__ __forceinline__ void block_range(int n, int &c0, int &c1) {
     c1 = (int)(((long long)n * (blockIdx.x + 1)) / gridDim.x);
 }
 
-// cell(c, x, wE, wN, wNE, wNW) for every cell c of this block's range of a
-// level; over the stencil window of the current sub-range, x[k] = val(k) and
-// the four slot weights are staged (FP64) in shared memory, all with
-// independent loads issued together.  Ends with a block barrier.
 __device__ unsigned long long *g_stage_trace;  // diagnostics: block 0 stamps staging / compute ends
 __device__ int g_stage_trace_n;
 __device__ int g_stage_trace_all;  // 1: every block records, mark | block << 16
@@ -102,21 +98,25 @@ __device__ __forceinline__ void stage_mark(int mark) {
     }
 }
 
+// Inputs of a cell of the block's own range: a, b, c are staged in shared
+// memory for the compute loop; d stays in the staging thread (for commit).
 struct Own {
-    float a, b, c;
+    float a, b, c, d;
 };
 
 // cell(c, x, wE, wN, wNE, wNW, rsum, r0, o) for every cell c of this block's
 // range of a level.  Over the stencil window of the current sub-range, x[k] =
-// val(k) and the four slot weights are staged (FP64) in shared memory, and
-// own(k) (up to three FP32 inputs of the cell itself) for the cells of the
-// sub-range.  The links that leave a face (boundary-ring cells) are summed in
-// the staging pass as well, one thread per link and a fixed-order 8-lane tree
-// per ring cell: rsum[ring rank - r0] = sum_k w_k (val(c) - val(nb_k)).  All
-// global loads happen while staging, where they are independent, so the
-// compute loop reads shared memory only.  Ends with a block barrier.
-template <class Val, class OwnF, class Cell>
-__device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val, OwnF own, Cell cell) {
+// load(k, mine, o) and the four slot weights are staged (FP64) in shared
+// memory; for the cells of the sub-range (mine) load also fills o, whose a, b,
+// c are staged too, and commit(k, o) then performs the cell's side effects
+// (global stores) after the loads of the pass are issued.  load must not
+// store.  The links that leave a face (boundary-ring cells) are summed while
+// staging as well: rsum[ring rank - r0] = sum_k w_k (x(c) - x(nb_k)), one
+// thread per ring cell.  All global loads happen while staging, where they are
+// independent, so the compute loop reads shared memory only.  Ends with a
+// block barrier.
+template <class Load, class Commit, class Cell>
+__device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load load, Commit commit, Cell cell) {
     const int N = S.N, n = S.n, nring = S.nring, bs = blockDim.x, tid = threadIdx.x;
     int c0, c1;
     block_range(n, c0, c1);
@@ -157,20 +157,23 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val
             fw1 = __ldg(rw4 + 2 * tid + 1);
             int f, i, j;
             ring_cell_of_rank(r0 + tid, N, nring, f, i, j);
-            fvc = val((f * N + j) * N + i);
+            Own none;
+            fvc = load((f * N + j) * N + i, false, none);
         }
         // window: values and slot weights, two cells per thread per pass with
         // every global load of both issued before any shared-memory store
         for (int k = w0 + tid; k < w1; k += 2 * bs) {
             const int k2 = k + bs;
             const bool two = k2 < w1;
+            const bool in1 = k >= s0 && k < s1, in2 = two && k2 >= s0 && k2 < s1;
+            Own o1{0.f, 0.f, 0.f, 0.f}, o2{0.f, 0.f, 0.f, 0.f};
             double e1 = 0, n1 = 0, ne1 = 0, nw1 = 0, v1 = 0;
             if (k >= 0 && k < n) {
                 e1 = __ldg(wd + k);
                 n1 = __ldg(wd + n + k);
                 ne1 = __ldg(wd + 2 * n + k);
                 nw1 = __ldg(wd + 3 * n + k);
-                v1 = val(k);
+                v1 = load(k, in1, o1);
             }
             double e2 = 0, n2 = 0, ne2 = 0, nw2 = 0, v2 = 0;
             if (two && k2 >= 0 && k2 < n) {
@@ -178,12 +181,10 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val
                 n2 = __ldg(wd + n + k2);
                 ne2 = __ldg(wd + 2 * n + k2);
                 nw2 = __ldg(wd + 3 * n + k2);
-                v2 = val(k2);
+                v2 = load(k2, in2, o2);
             }
-            const bool in1 = k >= s0 && k < s1, in2 = two && k2 >= s0 && k2 < s1;
-            Own o1{0.f, 0.f, 0.f}, o2{0.f, 0.f, 0.f};
-            if (in1) o1 = own(k);
-            if (in2) o2 = own(k2);
+            if (in1) commit(k, o1);
+            if (in2) commit(k2, o2);
             int q = k - w0;
             bx[q] = v1;
             b0[q] = e1;
@@ -228,13 +229,17 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Val val
                 w1v = __ldg(rw4 + 2 * q + 1);
                 int f, i, j;
                 ring_cell_of_rank(r0 + q, N, nring, f, i, j);
-                vc = val((f * N + j) * N + i);
+                Own none;
+                vc = load((f * N + j) * N + i, false, none);
             }
             const int o[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
             const float w[8] = {w0v.x, w0v.y, w0v.z, w0v.w, w1v.x, w1v.y, w1v.z, w1v.w};
             double v[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) v[k] = o[k] >= 0 ? val(o[k]) : vc;
+            for (int k = 0; k < 8; k++) {
+                Own none;
+                v[k] = o[k] >= 0 ? load(o[k], false, none) : vc;
+            }
             double t = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++)
@@ -270,41 +275,10 @@ __device__ __forceinline__ float presmooth_x(const LevelDev &L, int k, float b) 
     return (float)(kOmegaJ * __ldg(L.dinv + k) * b);
 }
 
-// Pre-smooth of a level from x = 0 with right-hand side b: x = w D^-1 b,
-// r = b - K x.
-__device__ __forceinline__ void phase_presmooth(const LevelDev &L, const float *b, double *buf) {
-    auto val = [&](int k) -> double { return (double)presmooth_x(L, k, b[k]); };
-    auto own = [&](int k) -> Own { return Own{b[k], 0.f, 0.f}; };
-    staged(L.S, buf, val, own, [&](int c, STAGED_ARGS) {
-        const float bc = o.a;
-        const float xc = (float)x[c];  // = presmooth_x(L, c, bc)
-        const double kx = APPLY(L.S, c, (double)xc);
-        L.x[c] = xc;
-        L.r[c] = (float)(bc - kx);
-    });
-}
-
-// Post-smooth: xo = x + w D^-1 (b - K x); returns sum dotr . xo when dotr != nullptr.
-__device__ __forceinline__ double phase_postsmooth(const LevelDev &L, const float *b, float *xo, const float *dotr,
-                                                   double *buf) {
-    double s = 0;
-    const float *xs = L.x;
-    auto val = [&](int k) -> double { return (double)xs[k]; };
-    auto own = [&](int k) -> Own { return Own{b[k], __ldg(L.dinv + k), dotr ? dotr[k] : 0.f}; };
-    staged(L.S, buf, val, own, [&](int c, STAGED_ARGS) {
-        const float xc = (float)x[c];
-        const float rc = (float)(o.a - APPLY(L.S, c, (double)xc));
-        const float out = xc + (float)(kOmegaJ * o.b * rc);
-        xo[c] = out;
-        s += (double)o.c * out;
-    });
-    return s;
-}
-
-// b_coarse = R r_fine.  Interior coarse cells gather their 4x4 fine window in
-// the CSR row order (fine index ascending) with the P weights; the others use
-// the CSR rows.
-__device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev &C, int c) {
+// (R r_fine) at coarse cell c.  Interior coarse cells gather their 4x4 fine
+// window in the CSR row order (fine index ascending) with the P weights; the
+// others use the CSR rows.
+__device__ __forceinline__ float restrict_value(const LevelDev &F, const LevelDev &C, int c) {
     const int Nc = C.S.N, Nf = F.S.N;
     int f, I, J;
     cell_fij(c, Nc, f, I, J);
@@ -328,11 +302,15 @@ __device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev 
         const int k0 = __ldg(F.rstart + c), k1 = __ldg(F.rstart + c + 1);
         for (int k = k0; k < k1; k++) acc += (double)(__ldg(F.rw + k) * F.r[__ldg(F.ridx + k)]);
     }
-    C.b[c] = (float)acc;
+    return (float)acc;
+}
+__device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev &C, int c) {
+    C.b[c] = restrict_value(F, C, c);
 }
 
-// x_fine += P xo_coarse.  Interior fine cells compute their 2x2 coarse taps.
-__device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &C, int i) {
+// x_fine + P xo_coarse at fine cell i.  Interior fine cells compute their 2x2
+// coarse taps.
+__device__ __forceinline__ float prolong_value(const LevelDev &F, const LevelDev &C, int i) {
     const int Nf = F.S.N, Nc = C.S.N;
     const float4 w = __ldg(reinterpret_cast<const float4 *>(F.pw) + i);
     const float *xc = C.xo;
@@ -353,7 +331,54 @@ __device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &
         t3 = t.w;
     }
     const float s = w.x * xc[t0] + w.y * xc[t1] + w.z * xc[t2] + w.w * xc[t3];
-    F.x[i] += (float)(kCorrScale * s);
+    return F.x[i] + (float)(kCorrScale * s);
+}
+__device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &C, int i) {
+    F.x[i] = prolong_value(F, C, i);
+}
+
+// Pre-smooth of a level from x = 0 with right-hand side b: x = w D^-1 b,
+// r = b - K x.
+__device__ __forceinline__ void phase_presmooth(const LevelDev &L, const float *b, double *buf) {
+    auto load = [&](int k, bool mine, Own &o) -> double {
+        const float bk = b[k];
+        if (mine) o.a = bk;
+        return (double)presmooth_x(L, k, bk);
+    };
+    auto commit = [&](int, const Own &) {};
+    staged(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
+        const float bc = o.a;
+        const float xc = (float)x[c];  // = presmooth_x(L, c, bc)
+        const double kx = APPLY(L.S, c, (double)xc);
+        L.x[c] = xc;
+        L.r[c] = (float)(bc - kx);
+    });
+}
+
+// Prolongation C -> L fused with L's post-smooth: x = x_L + P xo_C is formed on
+// the fly over the staged window (never stored), then xo = x + w D^-1 (b - K x);
+// returns sum dotr . xo when dotr != nullptr.  Same arithmetic as a separate
+// prolongation pass followed by the post-smooth, one grid barrier fewer.
+__device__ __forceinline__ double phase_prolong_postsmooth(const LevelDev &L, const LevelDev &C, const float *b,
+                                                           float *xo, const float *dotr, double *buf) {
+    double s = 0;
+    auto load = [&](int k, bool mine, Own &o) -> double {
+        if (mine) {
+            o.a = b[k];
+            o.b = __ldg(L.dinv + k);
+            o.c = dotr ? dotr[k] : 0.f;
+        }
+        return (double)prolong_value(L, C, k);
+    };
+    auto commit = [&](int, const Own &) {};
+    staged(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
+        const float xc = (float)x[c];
+        const float rc = (float)(o.a - APPLY(L.S, c, (double)xc));
+        const float out = xc + (float)(kOmegaJ * o.b * rc);
+        xo[c] = out;
+        s += (double)o.c * out;
+    });
+    return s;
 }
 
 // One damped-Jacobi sweep src -> dst with per-link conversions (small levels).
@@ -531,18 +556,15 @@ __device__ bool vcycle_rest(const SolveParams &P, const float *r, double *s_red,
             SYNC_OR(return false);
         }
     }
-    // up
+    // up: prolongation fused with each grid level's post-smooth
     for (int l = G - 1; l >= 0; l--) {
         const LevelDev &L = P.L[l];
-        GRID_LOOP(i, L.S.n) prolong_cell(L, P.L[l + 1], i);
-        trace_mark(P, 700 + l);
-        SYNC_OR(return false);
         if (l > 0) {
-            phase_postsmooth(L, L.b, L.xo, nullptr, buf);
+            phase_prolong_postsmooth(L, P.L[l + 1], L.b, L.xo, nullptr, buf);
             trace_mark(P, 900 + l);
             SYNC_OR(return false);
         } else {
-            double s = phase_postsmooth(L, r, P.z, r, buf);
+            double s = phase_prolong_postsmooth(L, P.L[1], r, P.z, r, buf);
             put_partial(P, RED_RZ, s, s_red);
             trace_mark(P, 900);
             SYNC_OR(return false);
@@ -638,9 +660,15 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     {
         double sb = 0, sr = 0;
         const float *psi = P.psi;
-        auto val = [&](int k) -> double { return (double)psi[k]; };
-        auto own = [&](int k) -> Own { return Own{P.omega[k], __ldg(P.area + k), 0.f}; };
-        staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+        auto load = [&](int k, bool mine, Own &o) -> double {
+            if (mine) {
+                o.a = P.omega[k];
+                o.b = __ldg(P.area + k);
+            }
+            return (double)psi[k];
+        };
+        auto commit = [&](int, const Own &) {};
+        staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
             double b = -(double)o.b * ((double)o.a - m2);
             double ri = b - APPLY(S0, c, x[c]);
             r[c] = (float)ri;
@@ -695,11 +723,11 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             const bool fst = first;
             const double be = beta;
             auto pnew = [&](int k) -> float { return fst ? z[k] : (float)(z[k] + be * po[k]); };
-            auto val = [&](int k) -> double { return (double)pnew(k); };
-            auto own = [&](int) -> Own { return Own{0.f, 0.f, 0.f}; };
+            auto load = [&](int k, bool, Own &) -> double { return (double)pnew(k); };
+            auto commit = [&](int, const Own &) {};
             double s = 0;
             float *pw = pn, *ap = P.Ap;
-            staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+            staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
                 const float pc = (float)x[c];
                 const double a = APPLY(S0, c, (double)pc);
                 pw[c] = pc;
@@ -727,13 +755,19 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             if (mg) {
                 // psi += alpha p; r' = r - alpha Ap; level-0 pre-smooth of r'
                 auto rnew = [&](int k) -> float { return (float)(ro[k] - alpha * Ap[k]); };
-                auto val = [&](int k) -> double { return (double)presmooth_x(L0, k, rnew(k)); };
-                // own: r, Ap of the cell; psi += alpha p happens here too (nothing else reads psi)
-                auto own = [&](int k) -> Own {
-                    P.psi[k] += (float)(alpha * pp[k]);
-                    return Own{ro[k], Ap[k], 0.f};
+                // mine: r, Ap of the cell staged; p and psi kept for commit,
+                // which does psi += alpha p (nothing else reads psi)
+                auto load = [&](int k, bool mine, Own &o) -> double {
+                    if (mine) {
+                        o.a = ro[k];
+                        o.b = Ap[k];
+                        o.c = pp[k];
+                        o.d = P.psi[k];
+                    }
+                    return (double)presmooth_x(L0, k, rnew(k));
                 };
-                staged(S0, buf, val, own, [&](int c, STAGED_ARGS) {
+                auto commit = [&](int k, const Own &o) { P.psi[k] = o.d + (float)(alpha * o.c); };
+                staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
                     const double ri = o.a - alpha * o.b;
                     const float rc = (float)ri;
                     rw_[c] = rc;
