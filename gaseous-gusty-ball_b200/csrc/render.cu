@@ -6,15 +6,19 @@
 // samples in ascending (particle index, sample k) order (upstream records are
 // binned thread-major over contiguous particle ranges, src/render.c:156-218).
 // This library reaches the same per-texel order without a global sort:
-//   1. count:  every particle counts the 32x32 texel tiles its arc touches
-//              (bounding box of its sample footprints per face) — atomics;
+//   1. count:  every particle reserves, on each 16x16 texel tile its arc may
+//              touch (FP32 conservative bound), one record slot per sample
+//              (FP32 upper bound on the sample count) — atomics;
 //   2. scan:   tile offsets (one block);
-//   3. fill:   every particle appends its index to the lists of those tiles;
-//   4. tiles:  one block per tile sorts its list (bitonic, ascending index),
-//              expands the samples of those particles that fall on the tile
-//              in (index, k) order, bins them per texel, sorts each texel's
-//              (short) list by sample order and applies the blends in order
-//              to the tile held in shared memory.
+//   3. fill:   every particle expands its samples exactly (FP64, as upstream)
+//              once and writes one record (order key, px, py) per (sample,
+//              tile) its footprint touches into that tile's slots;
+//   4. tiles:  one block per tile bins its records per texel, sorts each
+//              texel's few entries by order key and applies the blends in
+//              that order to the tile held in shared memory.  A tile whose
+//              records do not fit one shared-memory window is composited in
+//              consecutive key-range windows (found by a key histogram), each
+//              window complete before the next, which keeps the order.
 // The pending renormalisation of render_fade is fused into step 4.
 #include <algorithm>
 #include <atomic>
@@ -26,22 +30,23 @@
 
 namespace ggb {
 
-constexpr int kT = 32;              // tile edge in texels
-constexpr int kTB = 256;            // threads per tile block
-constexpr int kSortCap = 2048;      // tile lists up to this length sort in shared memory
-constexpr int kChunk = kTB;         // particles expanded per chunk
-constexpr int kSampleCap = 2048;    // samples binned per window
-constexpr int kEntryCap = 8192;     // (sample, texel) entries per window
+constexpr int kT = 16;              // tile edge in texels
 constexpr int kMaxSamples = 4096;   // upstream cap on samples per arc
+
+// One splat sample on one tile: its compositing order key (particle index
+// << 13 | sample k) and its texel-space centre on the tile's face.
+struct __align__(16) Rec {
+    unsigned long long key;
+    float px, py;
+};
 
 struct RenderPriv {
     int R = 0, ntx = 0, ntiles = 0;
     unsigned *tile_count = nullptr, *tile_start = nullptr, *tile_fill = nullptr;
-    unsigned *list = nullptr;
-    size_t list_cap = 0;
-    unsigned *slow_tiles = nullptr;  // tiles left to the sorted path
-    unsigned *slow_count = nullptr;
-    unsigned *total_host = nullptr;
+    Rec *recs = nullptr;
+    size_t rec_cap = 0;
+    unsigned *diag = nullptr;        // device: [0] windowed tiles of the last deposit, [1] slot overflow (sticky)
+    unsigned *total_host = nullptr;  // pinned: [0] reserved record slots, [1] slot overflow
     bool pending = false;
     float pending_scale = 1.f;
     float *mirror = nullptr;
@@ -182,21 +187,97 @@ __device__ __forceinline__ void arc_tiles_bound(const SplatCfg &C, D3 a, D3 b, E
     }
 }
 
+// Upper bound on arc_samples from FP32 arithmetic on the same inputs: the
+// FP32 angle differs from the FP64 one by orders of magnitude less than one
+// sample spacing, so ceil(angle / spacing) + 1 is never below the exact count.
+__device__ __forceinline__ unsigned arc_samples_bound(D3 a, D3 b, double spacing) {
+    const float ax = (float)a.x, ay = (float)a.y, az = (float)a.z, bx = (float)b.x, by = (float)b.y, bz = (float)b.z;
+    const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    const float ang = atan2f(sqrtf(cx * cx + cy * cy + cz * cz), ax * bx + ay * by + az * bz);
+    const float q = ang / (float)spacing;
+    if (!(q < (float)kMaxSamples)) return kMaxSamples;  // also NaN
+    return (unsigned)min(max((int)ceilf(q) + 1, 1), kMaxSamples);
+}
+
 __global__ void k_rd_count(int n, SplatCfg C, const float *prev, const float *pos, unsigned *tile_count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
-        arc_tiles_bound(C, a, b, [&](int t) { atomicAdd(tile_count + t, 1u); });
+        const unsigned nsb = arc_samples_bound(a, b, C.spacing);
+        arc_tiles_bound(C, a, b, [&](int t) { atomicAdd(tile_count + t, nsb); });
     }
 }
 
+// Samples of every arc (FP64, upstream src/render.c:87-131), one record per
+// (sample, face, tile) whose clamped footprint touches the tile.  A warp takes
+// 32 particles, computes their sample counts (one lane each), then spreads all
+// their samples evenly over its lanes (a warp prefix sum of the counts; each
+// lane finds the particle of its sample by a shuffle search), so particles with
+// many samples do not leave the other lanes idle.
 __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const unsigned *tile_start,
-                          unsigned *tile_fill, unsigned *list) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
-        arc_tiles_bound(C, a, b, [&](int t) {
-            unsigned slot = atomicAdd(tile_fill + t, 1u);
-            if (tile_start[t] + slot < tile_start[t + 1]) list[tile_start[t] + slot] = (unsigned)i;
-        });
+                          unsigned *tile_fill, Rec *recs, unsigned *diag) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int base = warp * 32; base < n; base += nwarps * 32) {
+        const int i = base + lane;
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, q0 = 0.f, q1 = 0.f, q2 = 0.f;
+        int ns = 0;
+        if (i < n) {
+            p0 = prev[3 * (size_t)i];
+            p1 = prev[3 * (size_t)i + 1];
+            p2 = prev[3 * (size_t)i + 2];
+            q0 = pos[3 * (size_t)i];
+            q1 = pos[3 * (size_t)i + 1];
+            q2 = pos[3 * (size_t)i + 2];
+            ns = arc_samples(d3(p0, p1, p2), d3(q0, q1, q2), C.spacing);
+        }
+        int incl = ns;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - ns;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            int j = 0;  // the last lane whose samples start at or before t
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int ex = __shfl_sync(0xffffffffu, excl, j + step);
+                if (t >= ex) j += step;
+            }
+            const int k = t - __shfl_sync(0xffffffffu, excl, j) + 1;
+            const int nsj = __shfl_sync(0xffffffffu, ns, j);
+            const D3 a = d3(__shfl_sync(0xffffffffu, p0, j), __shfl_sync(0xffffffffu, p1, j),
+                            __shfl_sync(0xffffffffu, p2, j));
+            const D3 b = d3(__shfl_sync(0xffffffffu, q0, j), __shfl_sync(0xffffffffu, q1, j),
+                            __shfl_sync(0xffffffffu, q2, j));
+            if (t >= total) continue;
+            const D3 d = arc_point(a, b, k, nsj);
+            const unsigned long long key = ((unsigned long long)(base + j) << 13) | (unsigned)k;
+#pragma unroll
+            for (int f = 0; f < 6; f++) {
+                float px, py;
+                if (!face_px(f, d, C.R, px, py)) continue;
+                const Box bx = footprint(px, py, C.rad, C.R);
+                if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) continue;
+                for (int ty = bx.ylo / kT; ty <= bx.yhi / kT; ty++)
+                    for (int tx = bx.xlo / kT; tx <= bx.xhi / kT; tx++) {
+                        const int tl = (f * C.ntx + ty) * C.ntx + tx;
+                        const unsigned slot = atomicAdd(tile_fill + tl, 1u);
+                        const unsigned s0 = __ldg(tile_start + tl);
+                        if (s0 + slot < __ldg(tile_start + tl + 1)) {
+                            Rec r;
+                            r.key = key;
+                            r.px = px;
+                            r.py = py;
+                            recs[s0 + slot] = r;
+                        } else {
+                            atomicOr(diag + 1, 1u);
+                        }
+                    }
+            }
+        }
     }
 }
 
@@ -227,401 +308,286 @@ __global__ void k_tile_scan(int n, const unsigned *cnt, unsigned *start, unsigne
     }
 }
 
-// Ascending sort of a[0..n) by the whole block (all-ascending bitonic network;
-// indices >= n act as +infinity).  `a` may be shared or global memory.
-__device__ void block_sort(unsigned *a, int n) {
-    int P = 1;
-    while (P < n) P <<= 1;
-    for (int k = 2; k <= P; k <<= 1) {
-        int half = k >> 1;
-        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-            int lo = (t / half) * k + (t % half);
-            int hi = lo ^ (k - 1);
-            if (hi < n) {
-                unsigned x = a[lo], y = a[hi];
-                if (x > y) {
-                    a[lo] = y;
-                    a[hi] = x;
-                }
-            }
-        }
-        __syncthreads();
-        for (int j = half >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                int lo = (t / j) * 2 * j + (t % j);
-                int hi = lo + j;
-                if (hi < n) {
-                    unsigned x = a[lo], y = a[hi];
-                    if (x > y) {
-                        a[lo] = y;
-                        a[hi] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
+// ---- tile compositing: one block per tile, one texel per thread ----------
+constexpr int kTB = kT * kT;   // threads per tile block: one texel each
+constexpr int kRec = 768;      // records of one window (shared memory)
+constexpr int kEnt = 2304;     // (record, texel) entries of one window
+constexpr int kHist = 1024;    // key buckets when a dense tile is cut into windows
+
+struct TileSmem {
+    union {
+        struct {
+            unsigned long long key[kRec];
+            float2 pos[kRec];
+        } r;
+        unsigned long long hist[kHist];  // window planning: entries << 32 | records per key bucket
+    } u;
+    float4 col[kRec];
+    unsigned short box[kRec];
+    unsigned short ent[kEnt];
+    int cnt[kT * kT];
+    int start[kT * kT];
+    unsigned long long scan_w[kTB / 32];
+    int cut;
+};
+
+struct TileGeo {
+    int x0, y0, tw, th;
+};
+
+constexpr unsigned short kNoBox = 0xffff;  // no texel of the tile has positive weight
+
+// The texels of the tile with positive tent weight for a sample at (px, py)
+// (upstream src/render.c:135-151) form a box (the tent is positive on an
+// interval per axis): x offset, y offset, width - 1, height - 1 in 4 bits each.
+__device__ __forceinline__ unsigned short rec_box(const SplatCfg &C, const TileGeo &G, float px, float py) {
+    const Box bx = footprint(px, py, C.rad, C.R);
+    int xa = max(bx.xlo, G.x0), xb = min(bx.xhi, G.x0 + G.tw - 1);
+    int ya = max(bx.ylo, G.y0), yb = min(bx.yhi, G.y0 + G.th - 1);
+    while (xa <= xb && !(__fmaf_rn(-fabsf((float)xa - px), C.invrad, 1.0f) > 0)) xa++;
+    while (xb >= xa && !(__fmaf_rn(-fabsf((float)xb - px), C.invrad, 1.0f) > 0)) xb--;
+    while (ya <= yb && !(__fmaf_rn(-fabsf((float)ya - py), C.invrad, 1.0f) > 0)) ya++;
+    while (yb >= ya && !(__fmaf_rn(-fabsf((float)yb - py), C.invrad, 1.0f) > 0)) yb--;
+    if (xa > xb || ya > yb) return kNoBox;
+    return (unsigned short)((xa - G.x0) | (ya - G.y0) << 4 | (xb - xa) << 8 | (yb - ya) << 12);
+}
+__device__ __forceinline__ int box_entries(unsigned short b) {
+    return b == kNoBox ? 0 : ((b >> 8 & 15) + 1) * ((b >> 12) + 1);
+}
+template <class F>
+__device__ __forceinline__ void box_texels(unsigned short b, F f) {
+    if (b == kNoBox) return;
+    const int x0 = b & 15, y0 = b >> 4 & 15, w = (b >> 8 & 15) + 1, h = (b >> 12) + 1;
+    for (int y = y0; y < y0 + h; y++)
+        for (int x = x0; x < x0 + w; x++) f(y * kT + x);
 }
 
-// Exclusive block scan of one int per thread (kTB threads); returns the total.
-__device__ __forceinline__ int block_excl_scan(int v, int &excl, int *s_w) {
+// Exclusive block scan of one value per thread (kTB threads); returns the total.
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long &excl,
+                                                              unsigned long long *s_w) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = v;
+    unsigned long long x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, x, o);
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) s_w[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < kTB / 32 ? s_w[lane] : 0;
+        unsigned long long w = lane < kTB / 32 ? s_w[lane] : 0ull;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, w, o);
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
         if (lane < kTB / 32) s_w[lane] = w;
     }
     __syncthreads();
-    int before = warp ? s_w[warp - 1] : 0;
-    int total = s_w[kTB / 32 - 1];
+    const unsigned long long before = warp ? s_w[warp - 1] : 0ull;
+    const unsigned long long total = s_w[kTB / 32 - 1];
     excl = before + x - v;
     __syncthreads();
     return total;
 }
 
-struct TileSmem {
-    float4 tex[kT * kT];
-    unsigned keys[kSortCap];
-    float4 col[kChunk];
-    float2 spos[kSampleCap];
-    unsigned short sp[kSampleCap];
-    int cnt[kT * kT];
-    int start[kT * kT];
-    unsigned short ent[kEntryCap];
-    int scan_w[kTB / 32];
-};
+// Record r with its box into slot s of the current window.
+__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box, const float4 *col) {
+    S.u.r.key[s] = r.key;
+    S.u.r.pos[s] = make_float2(r.px, r.py);
+    S.box[s] = box;
+    S.col[s] = col[r.key >> 13];
+}
 
-// One block per tile; see the file comment.
-__global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *prev, const float *pos, const float *col,
-                                                  const unsigned *tile_start, unsigned *list, float *buf,
-                                                  const unsigned *tiles, const unsigned *ntiles_p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
-    if (blockIdx.x >= *ntiles_p) return;
-    const int tile = (int)tiles[blockIdx.x];
-    const int R = C.R, ntx = C.ntx;
-    const int f = tile / (ntx * ntx), rem = tile - f * ntx * ntx, ty = rem / ntx, tx = rem - ty * ntx;
-    const int x0 = tx * kT, y0 = ty * kT;
-    const int tw = min(kT, R - x0), th = min(kT, R - y0);
-    const unsigned lstart = tile_start[tile];
-    const int cnt = (int)(tile_start[tile + 1] - lstart);
-    if (cnt == 0 && !C.renorm) return;
-    float4 *face = reinterpret_cast<float4 *>(buf) + (size_t)f * R * R;
-
-    for (int t = threadIdx.x; t < kT * kT; t += kTB) {
-        int lx = t % kT, ly = t / kT;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (lx < tw && ly < th) {
-            v = face[(size_t)(y0 + ly) * R + x0 + lx];
-            if (C.renorm) {
-                v.x *= C.scale;
-                v.y *= C.scale;
-                v.z *= C.scale;
-                v.w *= C.scale;
+// Composites the window's records [0, nw) into this thread's texel d, per
+// texel in ascending order key (every entry of the window fits: at most kEnt).
+__device__ __forceinline__ void composite_window(TileSmem &S, int nw, const SplatCfg &C, const TileGeo &G,
+                                                 float4 &d) {
+    const int q = threadIdx.x;
+    S.cnt[q] = 0;
+    __syncthreads();
+    for (int s = q; s < nw; s += kTB) box_texels(S.box[s], [&](int t) { atomicAdd(&S.cnt[t], 1); });
+    __syncthreads();
+    const int m = S.cnt[q];
+    unsigned long long ex;
+    block_excl_scan((unsigned long long)m, ex, S.scan_w);
+    S.start[q] = (int)ex;
+    S.cnt[q] = 0;
+    __syncthreads();
+    for (int s = q; s < nw; s += kTB)
+        box_texels(S.box[s], [&](int t) {
+            const int e = S.start[t] + atomicAdd(&S.cnt[t], 1);
+            if (e < kEnt) S.ent[e] = (unsigned short)s;
+        });
+    __syncthreads();
+    if (m) {
+        unsigned short *e = S.ent + (int)ex;
+        for (int v0 = 1; v0 < m; v0++) {
+            const unsigned short key = e[v0];
+            const unsigned long long kk = S.u.r.key[key];
+            int v = v0 - 1;
+            while (v >= 0 && S.u.r.key[e[v]] > kk) {
+                e[v + 1] = e[v];
+                v--;
             }
+            e[v + 1] = key;
         }
-        S.tex[t] = v;
-    }
-
-    // particle list of this tile, ascending
-    const unsigned *keys;
-    if (cnt <= kSortCap) {
-        for (int t = threadIdx.x; t < cnt; t += kTB) S.keys[t] = list[lstart + t];
-        __syncthreads();
-        block_sort(S.keys, cnt);
-        keys = S.keys;
-    } else {
-        block_sort(list + lstart, cnt);
-        keys = list + lstart;
+        const float invrad = C.invrad, invg = C.invg;
+        const float xf = (float)(G.x0 + q % kT), yf = (float)(G.y0 + q / kT);
+        for (int v = 0; v < m; v++) {
+            const int s = e[v];
+            const float2 pp = S.u.r.pos[s];
+            const float4 c = S.col[s];
+            const float w0 = C.alpha * c.w;
+            const float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
+            const float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
+            const float w = __fmul_rn(__fmul_rn(w0, wx), wy);
+            const float keep = 1.0f - w, add = __fmul_rn(w, invg);
+            d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
+            d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
+            d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
+            d.w = __fmaf_rn(d.w, keep, add);
+        }
     }
     __syncthreads();
+}
 
-    const float rad = C.rad, invrad = C.invrad, invg = C.invg;
-    // texels with positive tent weight per axis: < 2 rad + 1 (rounding of invrad included)
-    const int fpmax = (2 * (int)ceilf(rad) + 1) * (2 * (int)ceilf(rad) + 1);
-    const int win = max(1, min(kSampleCap, kEntryCap / max(1, fpmax)));
-
-    for (int c0 = 0; c0 < cnt; c0 += kChunk) {
-        const int t = threadIdx.x;
-        const bool valid = c0 + t < cnt;
-        D3 a = d3(0, 0, 0), b = d3(0, 0, 0);
-        int ns = 0, mine = 0;
-        if (valid) {
-            unsigned pidx = keys[c0 + t];
-            a = load3(prev + 3 * (size_t)pidx);
-            b = load3(pos + 3 * (size_t)pidx);
-            S.col[t] = reinterpret_cast<const float4 *>(col)[pidx];
-            ns = arc_samples(a, b, C.spacing);
-            for (int k = 1; k <= ns; k++) {
-                float px, py;
-                if (!face_px(f, arc_point(a, b, k, ns), R, px, py)) continue;
-                Box bx = footprint(px, py, rad, R);
-                if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) continue;
-                if (bx.xhi < x0 || bx.xlo >= x0 + tw || bx.yhi < y0 || bx.ylo >= y0 + th) continue;
-                mine++;
-            }
-        }
-        int first;
-        const int M = block_excl_scan(mine, first, S.scan_w);
-        for (int w0 = 0; w0 < M; w0 += win) {
-            const int w1 = min(M, w0 + win);
-            // samples of this window, in (particle, k) order
-            if (valid && mine > 0 && first < w1 && first + mine > w0) {
-                int s = first;
-                for (int k = 1; k <= ns && s < w1; k++) {
-                    float px, py;
-                    if (!face_px(f, arc_point(a, b, k, ns), R, px, py)) continue;
-                    Box bx = footprint(px, py, rad, R);
-                    if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) continue;
-                    if (bx.xhi < x0 || bx.xlo >= x0 + tw || bx.yhi < y0 || bx.ylo >= y0 + th) continue;
-                    if (s >= w0) {
-                        S.spos[s - w0] = make_float2(px, py);
-                        S.sp[s - w0] = (unsigned short)t;
-                    }
-                    s++;
-                }
-            }
-            for (int q = threadIdx.x; q < kT * kT; q += kTB) S.cnt[q] = 0;
-            __syncthreads();
-            const int ws = w1 - w0;
-            // count texel entries
-            for (int s = threadIdx.x; s < ws; s += kTB) {
-                float2 pp = S.spos[s];
-                Box bx = footprint(pp.x, pp.y, rad, R);
-                int xa = max(bx.xlo, x0), xb = min(bx.xhi, x0 + tw - 1);
-                int ya = max(bx.ylo, y0), yb = min(bx.yhi, y0 + th - 1);
-                for (int y = ya; y <= yb; y++) {
-                    float wy = __fmaf_rn(-fabsf((float)y - pp.y), invrad, 1.0f);
-                    if (wy <= 0) continue;
-                    for (int x = xa; x <= xb; x++) {
-                        float wx = __fmaf_rn(-fabsf((float)x - pp.x), invrad, 1.0f);
-                        if (wx <= 0) continue;
-                        atomicAdd(&S.cnt[(y - y0) * kT + (x - x0)], 1);
-                    }
-                }
-            }
-            __syncthreads();
-            // texel offsets (each thread scans 4 consecutive texels)
-            {
-                int base = threadIdx.x * 4;
-                int c4[4], sum = 0;
-                for (int u = 0; u < 4; u++) {
-                    c4[u] = S.cnt[base + u];
-                    sum += c4[u];
-                }
-                int ex;
-                block_excl_scan(sum, ex, S.scan_w);
-                for (int u = 0; u < 4; u++) {
-                    S.start[base + u] = ex;
-                    ex += c4[u];
-                    S.cnt[base + u] = 0;
-                }
-            }
-            __syncthreads();
-            // fill entries (order within a texel fixed below)
-            for (int s = threadIdx.x; s < ws; s += kTB) {
-                float2 pp = S.spos[s];
-                Box bx = footprint(pp.x, pp.y, rad, R);
-                int xa = max(bx.xlo, x0), xb = min(bx.xhi, x0 + tw - 1);
-                int ya = max(bx.ylo, y0), yb = min(bx.yhi, y0 + th - 1);
-                for (int y = ya; y <= yb; y++) {
-                    float wy = __fmaf_rn(-fabsf((float)y - pp.y), invrad, 1.0f);
-                    if (wy <= 0) continue;
-                    for (int x = xa; x <= xb; x++) {
-                        float wx = __fmaf_rn(-fabsf((float)x - pp.x), invrad, 1.0f);
-                        if (wx <= 0) continue;
-                        int q = (y - y0) * kT + (x - x0);
-                        int slot = atomicAdd(&S.cnt[q], 1);
-                        S.ent[S.start[q] + slot] = (unsigned short)s;
-                    }
-                }
-            }
-            __syncthreads();
-            // per texel: order its samples, then blend (upstream src/render.c:135-151)
-            for (int q = threadIdx.x; q < kT * kT; q += kTB) {
-                int e0 = S.start[q], m = S.cnt[q];
-                if (!m) continue;
-                unsigned short *e = S.ent + e0;
-                for (int u = 1; u < m; u++) {
-                    unsigned short key = e[u];
-                    int v = u - 1;
-                    while (v >= 0 && e[v] > key) {
-                        e[v + 1] = e[v];
-                        v--;
-                    }
-                    e[v + 1] = key;
-                }
-                const float xf = (float)(x0 + q % kT), yf = (float)(y0 + q / kT);
-                float4 d = S.tex[q];
-                for (int u = 0; u < m; u++) {
-                    int s = e[u];
-                    float2 pp = S.spos[s];
-                    float4 c = S.col[S.sp[s]];
-                    float w0 = C.alpha * c.w;
-                    float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
-                    float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
-                    float w = __fmul_rn(__fmul_rn(w0, wx), wy);
-                    float keep = 1.0f - w, add = __fmul_rn(w, invg);
-                    d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
-                    d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
-                    d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
-                    d.w = __fmaf_rn(d.w, keep, add);
-                }
-                S.tex[q] = d;
-            }
-            __syncthreads();
-        }
+// A tile whose records do not fit one window: consecutive key ranges [lo, hi),
+// each holding at most kRec records and kEnt entries, composited in turn.  hi
+// is the end of the longest run of key buckets (a histogram over [lo, top])
+// within both limits; when the first bucket alone is over, the search narrows
+// to that bucket.  One key is one record (a sample falls on a tile once), and
+// a record has at most 256 entries (its box lies on the tile), so every window
+// makes progress.
+__device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const float4 *col, const SplatCfg &C,
+                                   const TileGeo &G, float4 &d) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    unsigned long long kmin = ~0ull, kmax = 0;
+    for (int s = tid; s < m; s += kTB) {
+        const unsigned long long k = R[s].key;
+        kmin = min(kmin, k);
+        kmax = max(kmax, k);
     }
-
-    for (int t = threadIdx.x; t < kT * kT; t += kTB) {
-        int lx = t % kT, ly = t / kT;
-        if (lx < tw && ly < th) face[(size_t)(y0 + ly) * R + x0 + lx] = S.tex[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    }
+    if (tid < 2) S.u.hist[tid] = tid ? 0ull : ~0ull;
+    __syncthreads();
+    if (lane == 0) {
+        atomicMin(&S.u.hist[0], kmin);
+        atomicMax(&S.u.hist[1], kmax);
+    }
+    __syncthreads();
+    kmin = S.u.hist[0];
+    kmax = S.u.hist[1];
+    __syncthreads();
+    unsigned long long lo = kmin;
+    while (lo <= kmax) {
+        unsigned long long top = kmax, hi;
+        for (;;) {
+            const unsigned long long span = top - lo + 1, bw = (span + kHist - 1) / kHist;
+            for (int b = tid; b < kHist; b += kTB) S.u.hist[b] = 0;
+            if (tid == 0) S.cut = kHist;
+            __syncthreads();
+            for (int s = tid; s < m; s += kTB) {
+                const Rec r = R[s];
+                if (r.key < lo || r.key > top) continue;
+                const int e = box_entries(rec_box(C, G, r.px, r.py));
+                if (e) atomicAdd(&S.u.hist[(r.key - lo) / bw], ((unsigned long long)e << 32) | 1ull);
+            }
+            __syncthreads();
+            // first bucket at which the running totals pass a limit
+            constexpr int per = kHist / kTB;
+            unsigned long long mine = 0;
+            for (int u = 0; u < per; u++) mine += S.u.hist[tid * per + u];
+            unsigned long long run;
+            block_excl_scan(mine, run, S.scan_w);
+            for (int u = 0; u < per; u++) {
+                run += S.u.hist[tid * per + u];
+                if ((run >> 32) > (unsigned long long)kEnt || (run & 0xffffffffull) > (unsigned long long)kRec) {
+                    atomicMin(&S.cut, tid * per + u);
+                    break;
+                }
+            }
+            __syncthreads();
+            const int cut = S.cut;
+            __syncthreads();
+            if (cut > 0 || bw == 1) {
+                hi = lo + (unsigned long long)max(cut, 1) * bw;
+                if (hi > top + 1) hi = top + 1;
+                break;
+            }
+            top = lo + bw - 1;
+        }
+        if (tid == 0) S.cut = 0;  // reused as the window's record count
+        __syncthreads();
+        for (int s = tid; s < m; s += kTB) {
+            const Rec r = R[s];
+            if (r.key < lo || r.key >= hi) continue;
+            const unsigned short box = rec_box(C, G, r.px, r.py);
+            if (box == kNoBox) continue;
+            const int slot = atomicAdd(&S.cut, 1);
+            if (slot < kRec) window_put(S, slot, r, box, col);
+        }
+        __syncthreads();
+        const int nw = min(S.cut, kRec);
+        composite_window(S, nw, C, G, d);
+        lo = hi;
     }
 }
 
-// ---- fast per-tile path ------------------------------------------------
-// One pass over the tile's particles expands each arc's samples on this tile
-// (FP64, as upstream) and drops every (sample, texel) pair with positive tent
-// weight straight into that texel's fixed-size entry slots.  Each entry
-// carries the sample's global order key (particle index, k), and each texel
-// sorts its few entries by that key before blending, so neither the tile's
-// particle list nor the samples need any order.  A tile whose particles,
-// samples or per-texel entries exceed the fixed buffers is left untouched and
-// queued for k_rd_tiles (the sorted, windowed path).
-constexpr int kFastParticles = 512;
-constexpr int kFastSamples = 1536;
-constexpr int kTexelSlots = 12;
-
-struct FastSmem {
-    float4 col[kFastParticles];
-    float2 spos[kFastSamples];
-    unsigned long long skey[kFastSamples];
-    unsigned short sslot[kFastSamples];
-    unsigned short ent[kT * kT * kTexelSlots];
-    int tcnt[kT * kT];
-    int nsamp, overflow;
-};
-
-__global__ void __launch_bounds__(kTB) k_rd_tiles_fast(SplatCfg C, const float *prev, const float *pos,
-                                                       const float *col, const unsigned *tile_start,
-                                                       const unsigned *list, float *buf, unsigned *slow_tiles,
-                                                       unsigned *slow_count) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FastSmem &S = *reinterpret_cast<FastSmem *>(smem_raw);
-    const int tile = blockIdx.x;
+// One block per tile; see the file comment.
+__global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *col, const unsigned *tile_start,
+                                                  const unsigned *tile_fill, const Rec *recs, float *buf,
+                                                  unsigned *diag) {
+    __shared__ TileSmem S;
+    const int tile = blockIdx.x, q = threadIdx.x;
     const int R = C.R, ntx = C.ntx;
+    const unsigned s0 = __ldg(tile_start + tile);
+    const int m = (int)min(__ldg(tile_fill + tile), __ldg(tile_start + tile + 1) - s0);
+    if (m == 0 && !C.renorm) return;
     const int f = tile / (ntx * ntx), rem = tile - f * ntx * ntx, ty = rem / ntx, tx = rem - ty * ntx;
-    const int x0 = tx * kT, y0 = ty * kT;
-    const int tw = min(kT, R - x0), th = min(kT, R - y0);
-    const unsigned lstart = tile_start[tile];
-    const int cnt = (int)(tile_start[tile + 1] - lstart);
-    if (cnt == 0 && !C.renorm) return;
-    if (cnt > kFastParticles) {
-        if (threadIdx.x == 0) slow_tiles[atomicAdd(slow_count, 1u)] = (unsigned)tile;
-        return;
-    }
-    if (threadIdx.x == 0) {
-        S.nsamp = 0;
-        S.overflow = 0;
-    }
-    for (int q = threadIdx.x; q < kT * kT; q += kTB) S.tcnt[q] = 0;
-    __syncthreads();
-    const float rad = C.rad, invrad = C.invrad, invg = C.invg;
-    for (int u = threadIdx.x; u < cnt; u += kTB) {
-        unsigned pidx = list[lstart + u];
-        D3 a = load3(prev + 3 * (size_t)pidx), b = load3(pos + 3 * (size_t)pidx);
-        S.col[u] = reinterpret_cast<const float4 *>(col)[pidx];
-        int ns = arc_samples(a, b, C.spacing);
-        for (int k = 1; k <= ns; k++) {
-            float px, py;
-            if (!face_px(f, arc_point(a, b, k, ns), R, px, py)) continue;
-            Box bx = footprint(px, py, rad, R);
-            int xa = max(bx.xlo, x0), xb = min(bx.xhi, x0 + tw - 1);
-            int ya = max(bx.ylo, y0), yb = min(bx.yhi, y0 + th - 1);
-            if (xa > xb || ya > yb) continue;
-            int sidx = atomicAdd(&S.nsamp, 1);
-            if (sidx >= kFastSamples) {
-                S.overflow = 1;
-                break;
-            }
-            S.spos[sidx] = make_float2(px, py);
-            S.skey[sidx] = ((unsigned long long)pidx << 13) | (unsigned)k;
-            S.sslot[sidx] = (unsigned short)u;
-            for (int y = ya; y <= yb; y++) {
-                float wy = __fmaf_rn(-fabsf((float)y - py), invrad, 1.0f);
-                if (wy <= 0) continue;
-                for (int x = xa; x <= xb; x++) {
-                    float wx = __fmaf_rn(-fabsf((float)x - px), invrad, 1.0f);
-                    if (wx <= 0) continue;
-                    int q = (y - y0) * kT + (x - x0);
-                    int slot = atomicAdd(&S.tcnt[q], 1);
-                    if (slot < kTexelSlots)
-                        S.ent[q * kTexelSlots + slot] = (unsigned short)sidx;
-                    else
-                        S.overflow = 1;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    if (S.overflow) {
-        if (threadIdx.x == 0) slow_tiles[atomicAdd(slow_count, 1u)] = (unsigned)tile;
-        return;  // tile untouched; the sorted path redoes it
-    }
-    // per texel: order by (particle, k), then blend (upstream src/render.c:135-151)
+    TileGeo G;
+    G.x0 = tx * kT;
+    G.y0 = ty * kT;
+    G.tw = min(kT, R - G.x0);
+    G.th = min(kT, R - G.y0);
     float4 *face = reinterpret_cast<float4 *>(buf) + (size_t)f * R * R;
-    for (int q = threadIdx.x; q < kT * kT; q += kTB) {
-        const int lx = q % kT, ly = q / kT;
-        const int m = S.tcnt[q];
-        if (lx >= tw || ly >= th || (m == 0 && !C.renorm)) continue;
-        float4 *dp = face + (size_t)(y0 + ly) * R + x0 + lx;
-        float4 d = *dp;
+    const int lx = q % kT, ly = q / kT;
+    const bool inside = lx < G.tw && ly < G.th;
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (inside) {
+        d = face[(size_t)(G.y0 + ly) * R + G.x0 + lx];
         if (C.renorm) {
             d.x *= C.scale;
             d.y *= C.scale;
             d.z *= C.scale;
             d.w *= C.scale;
         }
-        unsigned short *e = S.ent + q * kTexelSlots;
-        for (int u = 1; u < m; u++) {
-            unsigned short key = e[u];
-            unsigned long long kk = S.skey[key];
-            int v = u - 1;
-            while (v >= 0 && S.skey[e[v]] > kk) {
-                e[v + 1] = e[v];
-                v--;
-            }
-            e[v + 1] = key;
-        }
-        const float xf = (float)(x0 + lx), yf = (float)(y0 + ly);
-        for (int u = 0; u < m; u++) {
-            int sdx = e[u];
-            float2 pp = S.spos[sdx];
-            float4 c = S.col[S.sslot[sdx]];
-            float w0 = C.alpha * c.w;
-            float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
-            float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
-            float w = __fmul_rn(__fmul_rn(w0, wx), wy);
-            float keep = 1.0f - w, add = __fmul_rn(w, invg);
-            d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
-            d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
-            d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
-            d.w = __fmaf_rn(d.w, keep, add);
-        }
-        *dp = d;
     }
+    if (m > 0) {
+        const Rec *Rt = recs + s0;
+        const float4 *col4 = reinterpret_cast<const float4 *>(col);
+        int e = 0;
+        if (m <= kRec)
+            for (int s = q; s < m; s += kTB) {
+                const Rec r = Rt[s];
+                const unsigned short box = rec_box(C, G, r.px, r.py);
+                window_put(S, s, r, box, col4);
+                e += box_entries(box);
+            }
+        unsigned long long ex;
+        const unsigned long long E = block_excl_scan((unsigned long long)e, ex, S.scan_w);
+        if (m <= kRec && E <= (unsigned long long)kEnt) {
+            composite_window(S, m, C, G, d);
+        } else {
+            if (q == 0) atomicAdd(diag, 1u);
+            composite_windowed(S, Rt, m, col4, C, G, d);
+        }
+    }
+    if (inside) face[(size_t)(G.y0 + ly) * R + G.x0 + lx] = d;
 }
 
 // Buffer renormalisation on its own (a second renormalisation falling due
@@ -660,9 +626,11 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
+    (void)sync_total;
     stage_begin(ST_BIN);
     GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
+    GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, sizeof(unsigned), s));
     unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
     if (n > 0) {
         k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
@@ -670,27 +638,24 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     }
     k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, Pv->tile_start, Pv->tile_count + Pv->ntiles);
     GGB_LAUNCHED();
-    (void)sync_total;
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     stage_end(ST_BIN);
     GGB_CHECK(cudaStreamSynchronize(s));
-    size_t need = *Pv->total_host;
-    if (need > Pv->list_cap) {
-        dev_free(Pv->list);
-        Pv->list_cap = need + need / 4 + 1024;
-        Pv->list = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->list_cap);
+    if (Pv->total_host[1])
+        fail_msg("render_deposit: a tile's sample records exceeded the slots reserved for them (internal error)");
+    size_t need = Pv->total_host[0];
+    if (need > Pv->rec_cap) {
+        dev_free(Pv->recs);
+        Pv->rec_cap = need + need / 4 + 1024;
+        Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
     }
     stage_begin(ST_TILES);
     if (n > 0) {
-        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->list);
+        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->diag);
         GGB_LAUNCHED();
     }
-    GGB_CHECK(cudaMemsetAsync(Pv->slow_count, 0, sizeof(unsigned), s));
-    k_rd_tiles_fast<<<Pv->ntiles, kTB, sizeof(FastSmem), s>>>(C, P->prev, P->pos, P->col, Pv->tile_start, Pv->list,
-                                                               r->buf, Pv->slow_tiles, Pv->slow_count);
-    GGB_LAUNCHED();
-    k_rd_tiles<<<Pv->ntiles, kTB, sizeof(TileSmem), s>>>(C, P->prev, P->pos, P->col, Pv->tile_start, Pv->list,
-                                                           r->buf, Pv->slow_tiles, Pv->slow_count);
+    k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, P->col, Pv->tile_start, Pv->tile_fill, Pv->recs, r->buf, Pv->diag);
     GGB_LAUNCHED();
     stage_end(ST_TILES);
     Pv->pending = false;
@@ -742,11 +707,9 @@ GGB_EXPORT int render_init(Render *r, int R, float radius, float alpha) {
     Pv->tile_count = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_start = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_fill = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
-    Pv->slow_tiles = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
-    Pv->slow_count = (unsigned *)dev_alloc(sizeof(unsigned));
-    GGB_CHECK(cudaMallocHost(&Pv->total_host, sizeof(unsigned)));
-    GGB_CHECK(cudaFuncSetAttribute(k_rd_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
-    GGB_CHECK(cudaFuncSetAttribute(k_rd_tiles_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FastSmem)));
+    Pv->diag = (unsigned *)dev_alloc(sizeof(unsigned) * 2);
+    GGB_CHECK(cudaMallocHost(&Pv->total_host, sizeof(unsigned) * 2));
+    Pv->total_host[0] = Pv->total_host[1] = 0;
     r->tr = reinterpret_cast<ThreadRecs *>(Pv);
     sync();
     return 0;
@@ -759,9 +722,8 @@ GGB_EXPORT void render_free(Render *r) {
         dev_free(Pv->tile_count);
         dev_free(Pv->tile_start);
         dev_free(Pv->tile_fill);
-        dev_free(Pv->slow_tiles);
-        dev_free(Pv->slow_count);
-        dev_free(Pv->list);
+        dev_free(Pv->diag);
+        dev_free(Pv->recs);
         cudaFreeHost(Pv->total_host);
         if (Pv->mirror) cudaFreeHost(Pv->mirror);
         delete Pv;
@@ -856,14 +818,14 @@ GGB_EXPORT void ggb_render_read(const Render *r, float *out) {
     for (size_t i = 0; i < n; i++) out[i] = Pv->pending ? (Pv->mirror[i] * sc) * g : Pv->mirror[i] * g;
 }
 
-// Diagnostics: tiles of the last deposit (all tiles, and those that took the
-// sorted fallback path) and the number of (particle, tile) list entries.
+// Diagnostics of the last deposit: all tiles, the tiles composited in several
+// key-range windows, and the record slots reserved for (sample, tile) records.
 GGB_EXPORT void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, unsigned *entries) {
     RenderPriv *Pv = rpriv(r);
     sync();
     unsigned sc = 0;
-    GGB_CHECK(cudaMemcpy(&sc, Pv->slow_count, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    GGB_CHECK(cudaMemcpy(&sc, Pv->diag, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (ntiles) *ntiles = (unsigned)Pv->ntiles;
     if (slow_tiles) *slow_tiles = sc;
-    if (entries) *entries = *Pv->total_host;
+    if (entries) *entries = Pv->total_host[0];
 }
