@@ -34,10 +34,12 @@ constexpr int kT = 16;              // tile edge in texels
 constexpr int kMaxSamples = 4096;   // upstream cap on samples per arc
 
 // One splat sample on one tile: its compositing order key (particle index
-// << 13 | sample k) and its texel-space centre on the tile's face.
+// << 13 | sample k), its texel-space centre on the tile's face and the
+// particle's colour (32 bytes: one DRAM sector).
 struct __align__(16) Rec {
     unsigned long long key;
     float px, py;
+    float4 col;
 };
 
 struct RenderPriv {
@@ -60,7 +62,7 @@ static RenderPriv *rpriv(const Render *r) {
 }
 
 struct SplatCfg {
-    int R, ntx;
+    int R, ntx, ntiles;
     float rad, invrad, invg, alpha;
     double spacing;
     int renorm;
@@ -80,6 +82,24 @@ __device__ __forceinline__ D3 arc_point(D3 a, D3 b, int k, int ns) {
 __device__ __forceinline__ int arc_samples(D3 a, D3 b, double spacing) {
     int ns = (int)ceil(angle(a, b) / spacing);
     return ns < 1 ? 1 : (ns > kMaxSamples ? kMaxSamples : ns);
+}
+
+// arc_samples for FP32 endpoints, the same value with less work: the FP32
+// quotient q = angle / spacing differs from the FP64 one by less than
+// err = 2e-6 (1 / spacing + q) + 1e-4 (the FP32 cross and dot products of
+// unit vectors are off by ~2e-7 absolute, atan2f by 2 ulp, the division by
+// half an ulp; err is twice their sum).  When q is farther than err from every
+// integer, ceil(q) is the FP64 ceiling; otherwise the FP64 path decides.
+__device__ __forceinline__ int arc_samples_f(float ax, float ay, float az, float bx, float by, float bz,
+                                             double spacing) {
+    const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+    const float q = atan2f(sqrtf(cx * cx + cy * cy + cz * cz), ax * bx + ay * by + az * bz) / (float)spacing;
+    if (q < (float)(kMaxSamples - 1)) {
+        const float err = 2e-6f * (1.0f / (float)spacing + q) + 1e-4f;
+        const float fl = floorf(q);
+        if (q - fl > err && fl + 1.0f - q > err) return (int)fl + 1;
+    }
+    return arc_samples(d3(ax, ay, az), d3(bx, by, bz), spacing);
 }
 
 // Projection of d on face f: false when the face is not used for d
@@ -207,19 +227,83 @@ __global__ void k_rd_count(int n, SplatCfg C, const float *prev, const float *po
     }
 }
 
+// The face of the largest |component| of d (its d.c >= 1/sqrt(3) > 0.5, so
+// upstream src/render.c:92-98 always draws the sample there) as dc, dr, du
+// exactly as face_proj(f) gives them.
+__device__ __forceinline__ int primary_face(D3 d, double &dc, double &dr, double &du) {
+    const double ax = fabs(d.x), ay = fabs(d.y), az = fabs(d.z);
+    if (az >= ax && az >= ay) {
+        if (d.z >= 0) { dc = d.z; dr = d.x; du = d.y; return 0; }
+        dc = -d.z; dr = -d.x; du = d.y; return 2;
+    }
+    if (ax >= ay) {
+        if (d.x >= 0) { dc = d.x; dr = -d.z; du = d.y; return 1; }
+        dc = -d.x; dr = d.z; du = d.y; return 3;
+    }
+    if (d.y >= 0) { dc = d.y; dr = d.x; du = -d.z; return 4; }
+    dc = -d.y; dr = d.x; du = d.z; return 5;
+}
+
+// Appends record r to tile tl.  Lanes of the warp that append to the same
+// tile share one atomic (the lowest such lane adds the group's count).
+__device__ __forceinline__ void append_rec(int tl, bool active, const Rec &r, const unsigned *tile_start,
+                                           unsigned *tile_fill, Rec *recs, unsigned *diag) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const unsigned grp = __match_any_sync(act, tl);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(tile_fill + tl, (unsigned)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const unsigned slot = base + __popc(grp & ((1u << lane) - 1u));
+    const unsigned s0 = __ldg(tile_start + tl);
+    if (s0 + slot < __ldg(tile_start + tl + 1))
+        recs[s0 + slot] = r;
+    else
+        atomicOr(diag + 1, 1u);
+}
+
+// Records of one (sample, face): one per tile its clamped footprint touches.
+__device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, float py, bool active,
+                                          unsigned long long key, float4 col, const unsigned *tile_start,
+                                          unsigned *tile_fill, Rec *recs, unsigned *diag) {
+    Box bx = footprint(px, py, C.rad, C.R);
+    if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) active = false;
+    const int tx0 = bx.xlo / kT, ty0 = bx.ylo / kT;
+    const int ntxs = active ? bx.xhi / kT - tx0 + 1 : 0, ntys = active ? bx.yhi / kT - ty0 + 1 : 0;
+    int most = ntxs * ntys;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) most = max(most, __shfl_xor_sync(0xffffffffu, most, o));
+    Rec r;
+    r.key = key;
+    r.px = px;
+    r.py = py;
+    r.col = col;
+    for (int u = 0; u < most; u++) {
+        const bool on = u < ntxs * ntys;
+        const int tl = on ? (f * C.ntx + ty0 + u / ntxs) * C.ntx + tx0 + u % ntxs : 0;
+        append_rec(tl, on, r, tile_start, tile_fill, recs, diag);
+    }
+}
+
 // Samples of every arc (FP64, upstream src/render.c:87-131), one record per
 // (sample, face, tile) whose clamped footprint touches the tile.  A warp takes
 // 32 particles, computes their sample counts (one lane each), then spreads all
 // their samples evenly over its lanes (a warp prefix sum of the counts; each
 // lane finds the particle of its sample by a shuffle search), so particles with
-// many samples do not leave the other lanes idle.
-__global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const unsigned *tile_start,
-                          unsigned *tile_fill, Rec *recs, unsigned *diag) {
+// many samples do not leave the other lanes idle.  Every sample is drawn on
+// its primary face in lock-step; the other faces with d.c >= 0.5 (near cube
+// edges only) follow.
+__global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const float *col,
+                          const unsigned *tile_start, unsigned *tile_fill, Rec *recs, size_t cap, unsigned *diag) {
+    if (tile_start[C.ntiles] > cap) return;  // the host grows the record buffer and runs this again
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const float4 *col4 = reinterpret_cast<const float4 *>(col);
     for (int base = warp * 32; base < n; base += nwarps * 32) {
         const int i = base + lane;
         float p0 = 0.f, p1 = 0.f, p2 = 0.f, q0 = 0.f, q1 = 0.f, q2 = 0.f;
+        float4 ci = make_float4(0.f, 0.f, 0.f, 0.f);
         int ns = 0;
         if (i < n) {
             p0 = prev[3 * (size_t)i];
@@ -228,7 +312,8 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
             q0 = pos[3 * (size_t)i];
             q1 = pos[3 * (size_t)i + 1];
             q2 = pos[3 * (size_t)i + 2];
-            ns = arc_samples(d3(p0, p1, p2), d3(q0, q1, q2), C.spacing);
+            ci = col4[i];
+            ns = arc_samples_f(p0, p1, p2, q0, q1, q2, C.spacing);
         }
         int incl = ns;
 #pragma unroll
@@ -252,30 +337,34 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
                             __shfl_sync(0xffffffffu, p2, j));
             const D3 b = d3(__shfl_sync(0xffffffffu, q0, j), __shfl_sync(0xffffffffu, q1, j),
                             __shfl_sync(0xffffffffu, q2, j));
-            if (t >= total) continue;
-            const D3 d = arc_point(a, b, k, nsj);
+            const float4 cj = make_float4(__shfl_sync(0xffffffffu, ci.x, j), __shfl_sync(0xffffffffu, ci.y, j),
+                                          __shfl_sync(0xffffffffu, ci.z, j), __shfl_sync(0xffffffffu, ci.w, j));
+            const bool live = t < total;
+            const D3 d = arc_point(a, b, live ? k : 1, live ? nsj : 1);
             const unsigned long long key = ((unsigned long long)(base + j) << 13) | (unsigned)k;
+            double dc, dr, du;
+            const int f0 = primary_face(d, dc, dr, du);
+            {
+                const double u = dr / dc, v = du / dc;
+                const float px = (float)__fma_rn((u + 1.0) * 0.5, (double)C.R, -0.5);
+                const float py = (float)__fma_rn((1.0 - v) * 0.5, (double)C.R, -0.5);
+                emit_face(C, f0, px, py, live, key, cj, tile_start, tile_fill, recs, diag);
+            }
+            // other faces with d.c >= 0.5 (cube edges and corners)
+            bool more = false;
 #pragma unroll
             for (int f = 0; f < 6; f++) {
-                float px, py;
-                if (!face_px(f, d, C.R, px, py)) continue;
-                const Box bx = footprint(px, py, C.rad, C.R);
-                if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) continue;
-                for (int ty = bx.ylo / kT; ty <= bx.yhi / kT; ty++)
-                    for (int tx = bx.xlo / kT; tx <= bx.xhi / kT; tx++) {
-                        const int tl = (f * C.ntx + ty) * C.ntx + tx;
-                        const unsigned slot = atomicAdd(tile_fill + tl, 1u);
-                        const unsigned s0 = __ldg(tile_start + tl);
-                        if (s0 + slot < __ldg(tile_start + tl + 1)) {
-                            Rec r;
-                            r.key = key;
-                            r.px = px;
-                            r.py = py;
-                            recs[s0 + slot] = r;
-                        } else {
-                            atomicOr(diag + 1, 1u);
-                        }
-                    }
+                double ec, er, eu;
+                face_proj(f, d, ec, er, eu);
+                more |= f != f0 && ec >= 0.5;
+            }
+            if (__any_sync(0xffffffffu, live && more)) {
+                for (int f = 0; f < 6; f++) {
+                    float px = 0.f, py = 0.f;
+                    const bool on = live && f != f0 && face_px(f, d, C.R, px, py);
+                    if (__any_sync(0xffffffffu, on))
+                        emit_face(C, f, px, py, on, key, cj, tile_start, tile_fill, recs, diag);
+                }
             }
         }
     }
@@ -328,7 +417,8 @@ struct TileSmem {
     int cnt[kT * kT];
     int start[kT * kT];
     unsigned long long scan_w[kTB / 32];
-    int cut;
+    int wsum[kTB / 32];
+    int cut, tot;
 };
 
 struct TileGeo {
@@ -392,11 +482,61 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
 }
 
 // Record r with its box into slot s of the current window.
-__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box, const float4 *col) {
+__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box) {
     S.u.r.key[s] = r.key;
     S.u.r.pos[s] = make_float2(r.px, r.py);
     S.box[s] = box;
-    S.col[s] = col[r.key >> 13];
+    S.col[s] = r.col;
+}
+
+// Blends the sorted entries e[0..m) of texel q into d (upstream
+// src/render.c:135-151).
+__device__ __forceinline__ void blend_texel(const TileSmem &S, unsigned short *e, int m, int q, const SplatCfg &C,
+                                            const TileGeo &G, float4 &d) {
+    for (int v0 = 1; v0 < m; v0++) {
+        const unsigned short key = e[v0];
+        const unsigned long long kk = S.u.r.key[key];
+        int v = v0 - 1;
+        while (v >= 0 && S.u.r.key[e[v]] > kk) {
+            e[v + 1] = e[v];
+            v--;
+        }
+        e[v + 1] = key;
+    }
+    const float invrad = C.invrad, invg = C.invg;
+    const float xf = (float)(G.x0 + q % kT), yf = (float)(G.y0 + q / kT);
+    for (int v = 0; v < m; v++) {
+        const int s = e[v];
+        const float2 pp = S.u.r.pos[s];
+        const float4 c = S.col[s];
+        const float w0 = C.alpha * c.w;
+        const float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
+        const float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
+        const float w = __fmul_rn(__fmul_rn(w0, wx), wy);
+        const float keep = 1.0f - w, add = __fmul_rn(w, invg);
+        d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
+        d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
+        d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
+        d.w = __fmaf_rn(d.w, keep, add);
+    }
+}
+
+// Exclusive scan over the block of one count per thread with one barrier:
+// a warp scan, the warp totals through shared memory, then each thread adds
+// the totals of the warps before its own.
+__device__ __forceinline__ int block_scan_1sync(int c, int *wsum) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    return before + incl - c;
 }
 
 // Composites the window's records [0, nw) into this thread's texel d, per
@@ -420,35 +560,7 @@ __device__ __forceinline__ void composite_window(TileSmem &S, int nw, const Spla
             if (e < kEnt) S.ent[e] = (unsigned short)s;
         });
     __syncthreads();
-    if (m) {
-        unsigned short *e = S.ent + (int)ex;
-        for (int v0 = 1; v0 < m; v0++) {
-            const unsigned short key = e[v0];
-            const unsigned long long kk = S.u.r.key[key];
-            int v = v0 - 1;
-            while (v >= 0 && S.u.r.key[e[v]] > kk) {
-                e[v + 1] = e[v];
-                v--;
-            }
-            e[v + 1] = key;
-        }
-        const float invrad = C.invrad, invg = C.invg;
-        const float xf = (float)(G.x0 + q % kT), yf = (float)(G.y0 + q / kT);
-        for (int v = 0; v < m; v++) {
-            const int s = e[v];
-            const float2 pp = S.u.r.pos[s];
-            const float4 c = S.col[s];
-            const float w0 = C.alpha * c.w;
-            const float wy = __fmaf_rn(-fabsf(yf - pp.y), invrad, 1.0f);
-            const float wx = __fmaf_rn(-fabsf(xf - pp.x), invrad, 1.0f);
-            const float w = __fmul_rn(__fmul_rn(w0, wx), wy);
-            const float keep = 1.0f - w, add = __fmul_rn(w, invg);
-            d.x = __fmaf_rn(d.x, keep, __fmul_rn(add, c.x));
-            d.y = __fmaf_rn(d.y, keep, __fmul_rn(add, c.y));
-            d.z = __fmaf_rn(d.z, keep, __fmul_rn(add, c.z));
-            d.w = __fmaf_rn(d.w, keep, add);
-        }
-    }
+    if (m) blend_texel(S, S.ent + (int)ex, m, q, C, G, d);
     __syncthreads();
 }
 
@@ -459,8 +571,8 @@ __device__ __forceinline__ void composite_window(TileSmem &S, int nw, const Spla
 // to that bucket.  One key is one record (a sample falls on a tile once), and
 // a record has at most 256 entries (its box lies on the tile), so every window
 // makes progress.
-__device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const float4 *col, const SplatCfg &C,
-                                   const TileGeo &G, float4 &d) {
+__device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const SplatCfg &C, const TileGeo &G,
+                                   float4 &d) {
     const int tid = threadIdx.x, lane = tid & 31;
     unsigned long long kmin = ~0ull, kmax = 0;
     for (int s = tid; s < m; s += kTB) {
@@ -529,7 +641,7 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const float
             const unsigned short box = rec_box(C, G, r.px, r.py);
             if (box == kNoBox) continue;
             const int slot = atomicAdd(&S.cut, 1);
-            if (slot < kRec) window_put(S, slot, r, box, col);
+            if (slot < kRec) window_put(S, slot, r, box);
         }
         __syncthreads();
         const int nw = min(S.cut, kRec);
@@ -539,9 +651,10 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const float
 }
 
 // One block per tile; see the file comment.
-__global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *col, const unsigned *tile_start,
-                                                  const unsigned *tile_fill, const Rec *recs, float *buf,
-                                                  unsigned *diag) {
+__global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const unsigned *tile_start,
+                                                  const unsigned *tile_fill, const Rec *recs, size_t cap,
+                                                  float *buf, unsigned *diag) {
+    if (tile_start[C.ntiles] > cap) return;  // records not filled: see k_rd_fill
     __shared__ TileSmem S;
     const int tile = blockIdx.x, q = threadIdx.x;
     const int R = C.R, ntx = C.ntx;
@@ -569,22 +682,41 @@ __global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const float *col, 
     }
     if (m > 0) {
         const Rec *Rt = recs + s0;
-        const float4 *col4 = reinterpret_cast<const float4 *>(col);
-        int e = 0;
-        if (m <= kRec)
+        // one window: records and per-texel counts in one pass
+        S.cnt[q] = 0;
+        if (q == 0) S.tot = 0;
+        __syncthreads();
+        if (m <= kRec) {
+            int e = 0;
             for (int s = q; s < m; s += kTB) {
                 const Rec r = Rt[s];
                 const unsigned short box = rec_box(C, G, r.px, r.py);
-                window_put(S, s, r, box, col4);
+                window_put(S, s, r, box);
+                box_texels(box, [&](int t) { atomicAdd(&S.cnt[t], 1); });
                 e += box_entries(box);
             }
-        unsigned long long ex;
-        const unsigned long long E = block_excl_scan((unsigned long long)e, ex, S.scan_w);
-        if (m <= kRec && E <= (unsigned long long)kEnt) {
-            composite_window(S, m, C, G, d);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+            if ((q & 31) == 0 && e) atomicAdd(&S.tot, e);
+        }
+        __syncthreads();
+        if (m <= kRec && S.tot <= kEnt) {
+            const int c = S.cnt[q];
+            const int st = block_scan_1sync(c, S.wsum);
+            S.start[q] = st;
+            S.cnt[q] = 0;
+            __syncthreads();
+            for (int s = q; s < m; s += kTB)
+                box_texels(S.box[s], [&](int t) {
+                    const int e = S.start[t] + atomicAdd(&S.cnt[t], 1);
+                    if (e < kEnt) S.ent[e] = (unsigned short)s;
+                });
+            __syncthreads();
+            if (c) blend_texel(S, S.ent + st, c, q, C, G, d);
         } else {
             if (q == 0) atomicAdd(diag, 1u);
-            composite_windowed(S, Rt, m, col4, C, G, d);
+            __syncthreads();
+            composite_windowed(S, Rt, m, C, G, d);
         }
     }
     if (inside) face[(size_t)(G.y0 + ly) * R + G.x0 + lx] = d;
@@ -601,6 +733,7 @@ static SplatCfg splat_cfg(const Render *r, const RenderPriv *Pv) {
     SplatCfg C;
     C.R = r->R;
     C.ntx = Pv->ntx;
+    C.ntiles = Pv->ntiles;
     C.rad = r->radius;
     C.invrad = 1.0f / r->radius;
     C.invg = (float)(1.0 / r->g);
@@ -621,12 +754,31 @@ static void flush_pending(Render *r, RenderPriv *Pv) {
     Pv->dev_gen++;
 }
 
-void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
+// Fill and composite (after the count and scan of the same deposit).  Both
+// kernels do nothing when the reserved total exceeds the record buffer.
+static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, const SplatCfg &C) {
+    cudaStream_t s = stream();
+    const int n = P->n;
+    const unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
+    stage_begin(ST_TILES);
+    if (n > 0) {
+        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, P->col, Pv->tile_start, Pv->tile_fill, Pv->recs,
+                                     Pv->rec_cap, Pv->diag);
+        GGB_LAUNCHED();
+    }
+    k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->rec_cap, r->buf, Pv->diag);
+    GGB_LAUNCHED();
+    stage_end(ST_TILES);
+}
+
+// The whole deposit without a host round trip; returns after queueing it.
+// render_deposit checks, after its synchronisation, that the record buffer was
+// large enough, and otherwise grows it and repeats the fill and composite.
+void render_deposit_launch(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
-    (void)sync_total;
     stage_begin(ST_BIN);
     GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
@@ -638,26 +790,21 @@ void render_deposit_launch(Render *r, const Particles *P, bool sync_total) {
     }
     k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, Pv->tile_start, Pv->tile_count + Pv->ntiles);
     GGB_LAUNCHED();
+    stage_end(ST_BIN);
+    deposit_fill_tiles(r, P, Pv, C);
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    stage_end(ST_BIN);
     GGB_CHECK(cudaStreamSynchronize(s));
     if (Pv->total_host[1])
         fail_msg("render_deposit: a tile's sample records exceeded the slots reserved for them (internal error)");
-    size_t need = Pv->total_host[0];
+    const size_t need = Pv->total_host[0];
     if (need > Pv->rec_cap) {
         dev_free(Pv->recs);
         Pv->rec_cap = need + need / 4 + 1024;
         Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
+        GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
+        deposit_fill_tiles(r, P, Pv, C);
     }
-    stage_begin(ST_TILES);
-    if (n > 0) {
-        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->diag);
-        GGB_LAUNCHED();
-    }
-    k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, P->col, Pv->tile_start, Pv->tile_fill, Pv->recs, r->buf, Pv->diag);
-    GGB_LAUNCHED();
-    stage_end(ST_TILES);
     Pv->pending = false;
     Pv->pending_scale = 1.f;
     Pv->dev_gen++;
@@ -746,7 +893,7 @@ GGB_EXPORT void render_fade(Render *r, double fade) {
 }
 
 GGB_EXPORT void render_deposit(Render *r, const Particles *P) {
-    render_deposit_launch(r, P, true);
+    render_deposit_launch(r, P);
     sync();
 }
 
