@@ -370,30 +370,51 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
     }
 }
 
-// Exclusive scan of cnt[0..n) into start[0..n] (one block).
-__global__ void k_tile_scan(int n, const unsigned *cnt, unsigned *start, unsigned *total) {
-    __shared__ unsigned s_tot[1024];
-    const int T = blockDim.x, t = threadIdx.x;
-    int chunk = (n + T - 1) / T, lo = min(n, t * chunk), hi = min(n, lo + chunk);
-    unsigned s = 0;
-    for (int k = lo; k < hi; k++) s += cnt[k];
-    s_tot[t] = s;
-    __syncthreads();
-    if (t == 0) {
-        unsigned acc = 0;
-        for (int k = 0; k < T; k++) {
-            unsigned v = s_tot[k];
-            s_tot[k] = acc;
-            acc += v;
+// Exclusive scan of cnt[0..n) into start[0..n] (one block of 1024 threads).
+// The counts of up to 32 chunks of 1024 are loaded at once (coalesced, one
+// memory latency), then scanned chunk after chunk with warp shuffles.
+__global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, unsigned *start, unsigned *total) {
+    constexpr int kChunks = 32;
+    __shared__ unsigned s_w[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    unsigned carry = 0;
+    for (int g0 = 0; g0 < n; g0 += kChunks * 1024) {
+        unsigned v[kChunks];
+#pragma unroll
+        for (int c = 0; c < kChunks; c++) {
+            const int i = g0 + c * 1024 + t;
+            v[c] = i < n ? __ldg(cnt + i) : 0u;
         }
-        start[n] = acc;
-        *total = acc;
+#pragma unroll
+        for (int c = 0; c < kChunks; c++) {
+            if (g0 + c * 1024 >= n) break;
+            unsigned x = v[c];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_w[warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                unsigned w = s_w[lane];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                s_w[lane] = w;
+            }
+            __syncthreads();
+            const int i = g0 + c * 1024 + t;
+            if (i < n) start[i] = carry + (warp ? s_w[warp - 1] : 0u) + x - v[c];
+            carry += s_w[31];
+            __syncthreads();
+        }
     }
-    __syncthreads();
-    unsigned acc = s_tot[t];
-    for (int k = lo; k < hi; k++) {
-        start[k] = acc;
-        acc += cnt[k];
+    if (t == 0) {
+        start[n] = carry;
+        *total = carry;
     }
 }
 

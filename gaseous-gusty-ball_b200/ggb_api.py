@@ -142,6 +142,7 @@ class Api:
         for name, res, args in [
             ("ggb_launch_count", C.c_long, []),
             ("ggb_render_read", None, [P(T["Render"]), R]),
+            ("ggb_render_stats", None, [P(T["Render"]), P(C.c_uint), P(C.c_uint), P(C.c_uint)]),
             ("ggb_initial_velocity", None, [P(T["CubeSphere"]), P(InitParams), R, R]),
             ("drv_initial_velocity", None, [P(T["CubeSphere"]), P(InitParams), R, R]),
             ("drv_run", C.c_long, [P(T["CubeSphere"]), P(T["Fluid"]), P(T["Particles"]), P(T["Render"]),

@@ -153,7 +153,9 @@ def run(api, N, particles, R, steps, vel0, vband, forcing=0.5, rotation=3.0, tol
 
 
 def deposit(api, R, prev, pos, col, fade_steps=0, fade=0.02, radius=1.0, alpha=0.35):
-    """One render_deposit of given particle arcs (after `fade_steps` fades)."""
+    """One render_deposit of given particle arcs (after `fade_steps` fades).
+    With the GPU library, out["windowed"] is the number of tiles composited in
+    several key-range windows (ggb_render_stats)."""
     ps = G.ParticleSet(api, prev.shape[0])
     nr = api.np_real
     ps.array("prev", 3)[:] = prev.astype(nr)
@@ -164,6 +166,10 @@ def deposit(api, R, prev, pos, col, fade_steps=0, fade=0.02, radius=1.0, alpha=0
         sp.fade(fade)
     sp.deposit(ps)
     out = dict(faces=sp.faces(), g=np.array(sp.r.g))
+    if api.has("ggb_render_stats"):
+        nt, nw, ne = C.c_uint(), C.c_uint(), C.c_uint()
+        api.lib.ggb_render_stats(C.byref(sp.r), C.byref(nt), C.byref(nw), C.byref(ne))
+        out["windowed"] = nw.value
     sp.free()
     ps.free()
     return out

@@ -225,8 +225,9 @@ def test_deposit_cases(gpu, orc32, R, radius, max_angle, n):
     assert np.max(np.abs(a["faces"] - b["faces"]), initial=0.0) <= 1e-6
 
 
-def test_deposit_dense_tile_sorts_in_global_memory(gpu, orc32):
-    """> 2048 particles in one tile (the global-memory sort path)."""
+def test_deposit_dense_tile_key_windows(gpu, orc32):
+    """6000 particles on a few tiles: more records than one shared-memory
+    window holds, composited in several key-range windows."""
     rng = np.random.default_rng(11)
     n = 6000
     c = np.array([0.0, 0.0, 1.0])
@@ -237,12 +238,13 @@ def test_deposit_dense_tile_sorts_in_global_memory(gpu, orc32):
     col = rng.uniform(0.1, 1, size=(n, 4))
     a = K.deposit(gpu, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
     b = K.deposit(orc32, 64, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    assert a["windowed"] > 0
     assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
 
 
-def test_deposit_sample_overflow_takes_sorted_path(gpu, orc32):
-    """A tile whose particles are few (<= 1024) but whose samples overflow the
-    fast path's buffers (long arcs concentrated on one tile)."""
+def test_deposit_long_arcs_few_particles(gpu, orc32):
+    """500 particles whose long arcs pile many samples onto the same tiles
+    (more (record, texel) entries than one window holds)."""
     rng = np.random.default_rng(12)
     n = 500
     c = np.array([0.0, 0.0, 1.0])
