@@ -53,6 +53,10 @@ void stage_begin(int s);
 void stage_end(int s);
 void stage_collect();  // after a stream sync: accumulate the recorded intervals
 
+// The deferred renormalisation of render_fade (private state of a Render).
+void render_pending_get(const Render *r, int *pending, float *scale);
+void render_pending_set(Render *r, int pending, float scale);
+
 void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled
 void dev_free(void *p);
 void *managed_alloc(size_t bytes);  // cudaMallocManaged, zero-filled, resident on the device

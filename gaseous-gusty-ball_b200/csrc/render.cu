@@ -52,6 +52,8 @@ struct RenderPriv {
     bool pending = false;
     float pending_scale = 1.f;
     float *mirror = nullptr;
+    unsigned char *enc = nullptr;  // device scratch of the 8-bit encoders (host outputs)
+    size_t enc_cap = 0;
     std::atomic<unsigned long> dev_gen{1}, mirror_gen{0};
     std::mutex mu;
 };
@@ -843,6 +845,172 @@ static void refresh_mirror(const Render *r, RenderPriv *Pv) {
     Pv->mirror_gen.store(g);
 }
 
+void render_pending_get(const Render *r, int *pending, float *scale) {
+    const RenderPriv *Pv = rpriv(r);
+    *pending = Pv->pending ? 1 : 0;
+    *scale = Pv->pending_scale;
+}
+
+void render_pending_set(Render *r, int pending, float scale) {
+    RenderPriv *Pv = rpriv(r);
+    Pv->pending = pending != 0;
+    Pv->pending_scale = pending ? scale : 1.f;
+    Pv->dev_gen++;
+}
+
+// ---- 8-bit output encoding (upstream src/main.c:249-318) --------------------
+
+struct EncCfg {
+    int R, ch, has_bg, pending;
+    float g, pscale, bg[3];
+    int order[6];
+};
+
+// render_texel (upstream src/render.c:220-226), with a pending renormalisation
+// of render_fade applied first, as render_texel of this library does.
+__device__ __forceinline__ float4 enc_texel(const float4 *buf, const EncCfg &E, int f, int x, int y) {
+    float4 d = buf[((size_t)f * E.R + y) * E.R + x];
+    if (E.pending) {
+        d.x = __fmul_rn(d.x, E.pscale);
+        d.y = __fmul_rn(d.y, E.pscale);
+        d.z = __fmul_rn(d.z, E.pscale);
+        d.w = __fmul_rn(d.w, E.pscale);
+    }
+    return make_float4(__fmul_rn(d.x, E.g), __fmul_rn(d.y, E.g), __fmul_rn(d.z, E.g), __fmul_rn(d.w, E.g));
+}
+
+// to8 and render_pixel8 (upstream src/render.c:253-279), with the
+// contractions of the upstream gcc build (v * 255 + 0.5, c + bg (1 - a)).
+__device__ __forceinline__ unsigned char enc_u8(float v) {
+    if (v <= 0.f) return 0;
+    if (v >= 1.f) return 255;
+    return (unsigned char)__fmaf_rn(v, 255.0f, 0.5f);
+}
+__device__ __forceinline__ void enc_pixel8(float4 c, const EncCfg &E, unsigned char out[4]) {
+    float a = c.w;
+    a = a > 1.f ? 1.f : (a < 0.f ? 0.f : a);
+    if (!E.has_bg) {
+        if (a > 1e-6f) {
+            out[0] = enc_u8(__fdiv_rn(c.x, a));
+            out[1] = enc_u8(__fdiv_rn(c.y, a));
+            out[2] = enc_u8(__fdiv_rn(c.z, a));
+        } else {
+            out[0] = out[1] = out[2] = 0;
+        }
+        out[3] = enc_u8(a);
+    } else {
+        const float k = 1.0f - a;
+        out[0] = enc_u8(__fmaf_rn(E.bg[0], k, c.x));
+        out[1] = enc_u8(__fmaf_rn(E.bg[1], k, c.y));
+        out[2] = enc_u8(__fmaf_rn(E.bg[2], k, c.z));
+    }
+}
+
+__device__ __forceinline__ void enc_store(unsigned char *dst, const unsigned char px[4], int ch) {
+    for (int k = 0; k < ch; k++) dst[k] = px[k];
+}
+
+// The six faces (in the order E.order) as R x R images of ch channels.
+__global__ void k_enc_faces(EncCfg E, const float4 *buf, unsigned char *out) {
+    const int k = blockIdx.y, f = E.order[k];
+    const size_t np = (size_t)E.R * E.R;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(i / E.R), x = (int)(i - (size_t)y * E.R);
+        unsigned char px[4] = {0, 0, 0, 255};
+        enc_pixel8(enc_texel(buf, E, f, x, y), E, px);
+        enc_store(out + ((size_t)k * np + i) * E.ch, px, E.ch);
+    }
+}
+
+// The 4R x 3R cross net, RGBA (the caller clears it: cells without a face stay 0).
+__global__ void k_enc_net(EncCfg E, const float4 *buf, unsigned char *out) {
+    const int R = E.R, W = 4 * R;
+    const size_t np = (size_t)6 * R * R;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const int fy = (int)(i / R), x = (int)(i - (size_t)fy * R);
+        const int f = fy / R, y = fy - f * R;
+        const int cx = f < 4 ? f : 0, cy = f < 4 ? 1 : (f == 4 ? 0 : 2);
+        unsigned char px[4] = {0, 0, 0, 255};
+        enc_pixel8(enc_texel(buf, E, f, x, y), E, px);
+        enc_store(out + (((size_t)cy * R + y) * W + (size_t)cx * R + x) * 4, px, 4);
+    }
+}
+
+// The 2R x R equirectangular preview of ch channels: render_sample_dir
+// (upstream src/render.c:228-251) at the pixel centres' directions.
+__global__ void k_enc_preview(EncCfg E, const float4 *buf, unsigned char *out) {
+    const int R = E.R, W = 2 * R, H = R;
+    const size_t np = (size_t)W * H;
+    const double kPiD = 3.14159265358979323846;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(i / W), x = (int)(i - (size_t)y * W);
+        const double lat = __fma_rn(-((y + 0.5) / H), kPiD, kPiD / 2);
+        const double lon = __fma_rn((x + 0.5) / W * 2, kPiD, -kPiD);
+        const double cl = cos(lat);
+        const D3 d = d3(cl * sin(lon), sin(lat), cl * cos(lon));
+        const int f = face_of(d);
+        double dc, dr, du;
+        face_proj(f, d, dc, dr, du);
+        const double u = dr / dc, v = du / dc;
+        double px = __fma_rn((u + 1.0) * 0.5, (double)R, -0.5), py = __fma_rn((1.0 - v) * 0.5, (double)R, -0.5);
+        px = px < 0 ? 0 : (px > R - 1 ? R - 1 : px);
+        py = py < 0 ? 0 : (py > R - 1 ? R - 1 : py);
+        const int x0 = (int)px, y0 = (int)py;
+        const int x1 = x0 + 1 < R ? x0 + 1 : x0, y1 = y0 + 1 < R ? y0 + 1 : y0;
+        const float fx = (float)(px - x0), fy = (float)(py - y0);
+        const float4 a = enc_texel(buf, E, f, x0, y0), b = enc_texel(buf, E, f, x1, y0);
+        const float4 c = enc_texel(buf, E, f, x0, y1), e = enc_texel(buf, E, f, x1, y1);
+        const float gx = 1.0f - fx, gy = 1.0f - fy;
+        auto lerp2 = [&](float t00, float t10, float t01, float t11) {
+            const float lo = __fmaf_rn(gx, t00, __fmul_rn(fx, t10));
+            const float hi = __fmaf_rn(gx, t01, __fmul_rn(fx, t11));
+            return __fmaf_rn(gy, lo, __fmul_rn(fy, hi));
+        };
+        const float4 s = make_float4(lerp2(a.x, b.x, c.x, e.x), lerp2(a.y, b.y, c.y, e.y), lerp2(a.z, b.z, c.z, e.z),
+                                     lerp2(a.w, b.w, c.w, e.w));
+        unsigned char q[4] = {0, 0, 0, 255};
+        enc_pixel8(s, E, q);
+        enc_store(out + i * E.ch, q, E.ch);
+    }
+}
+
+static EncCfg enc_cfg(const Render *r, const RenderPriv *Pv, const float *bg) {
+    EncCfg E;
+    E.R = r->R;
+    E.has_bg = bg != nullptr;
+    E.ch = bg ? 3 : 4;
+    E.pending = Pv->pending ? 1 : 0;
+    E.pscale = Pv->pending_scale;
+    E.g = (float)r->g;
+    for (int k = 0; k < 3; k++) E.bg[k] = bg ? bg[k] : 0.f;
+    for (int k = 0; k < 6; k++) E.order[k] = k;
+    return E;
+}
+
+// Device destination of an encoder: out itself when the GPU can write it,
+// otherwise the cached scratch (copied to out by enc_finish).
+static unsigned char *enc_target(RenderPriv *Pv, unsigned char *out, size_t bytes, bool &staged) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, out) == cudaSuccess &&
+        (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged)) {
+        staged = false;
+        return out;
+    }
+    cudaGetLastError();
+    staged = true;
+    if (bytes > Pv->enc_cap) {
+        dev_free(Pv->enc);
+        Pv->enc = (unsigned char *)dev_alloc(bytes);
+        Pv->enc_cap = bytes;
+    }
+    return Pv->enc;
+}
+
+static void enc_finish(RenderPriv *Pv, unsigned char *out, size_t bytes, bool staged) {
+    if (staged) GGB_CHECK(cudaMemcpyAsync(out, Pv->enc, bytes, cudaMemcpyDeviceToHost, stream()));
+    sync();
+}
+
 }  // namespace ggb
 
 using namespace ggb;
@@ -894,6 +1062,7 @@ GGB_EXPORT void render_free(Render *r) {
         dev_free(Pv->recs);
         cudaFreeHost(Pv->total_host);
         if (Pv->mirror) cudaFreeHost(Pv->mirror);
+        dev_free(Pv->enc);
         delete Pv;
     }
     managed_free(r->buf);
@@ -996,4 +1165,58 @@ GGB_EXPORT void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *sl
     if (ntiles) *ntiles = (unsigned)Pv->ntiles;
     if (slow_tiles) *slow_tiles = sc;
     if (entries) *entries = Pv->total_host[0];
+}
+
+// Additive: the application driver's 8-bit images, encoded on the GPU (upstream
+// src/main.c:249-318).  bg == NULL: transparent (RGBA, un-premultiplied);
+// otherwise RGB over bg[3].  out: host or device memory.
+GGB_EXPORT int ggb_encode_faces(const Render *r, const float *bg, const int *face_order, unsigned char *out) {
+    RenderPriv *Pv = rpriv(r);
+    EncCfg E = enc_cfg(r, Pv, bg);
+    if (face_order) {
+        int seen = 0;
+        for (int k = 0; k < 6; k++) {
+            if (face_order[k] < 0 || face_order[k] > 5 || (seen >> face_order[k] & 1)) {
+                fprintf(stderr, "ggb_encode_faces: face_order must be a permutation of 0..5\n");
+                return -1;
+            }
+            seen |= 1 << face_order[k];
+            E.order[k] = face_order[k];
+        }
+    }
+    const size_t bytes = (size_t)6 * r->R * r->R * E.ch;
+    bool staged;
+    unsigned char *dst = enc_target(Pv, out, bytes, staged);
+    dim3 grid((unsigned)std::min<size_t>(((size_t)r->R * r->R + 255) / 256, 148 * 4), 6);
+    k_enc_faces<<<grid, 256, 0, stream()>>>(E, reinterpret_cast<const float4 *>(r->buf), dst);
+    GGB_LAUNCHED();
+    enc_finish(Pv, out, bytes, staged);
+    return 0;
+}
+
+GGB_EXPORT int ggb_encode_net(const Render *r, const float *bg, unsigned char *out) {
+    RenderPriv *Pv = rpriv(r);
+    EncCfg E = enc_cfg(r, Pv, bg);
+    const size_t bytes = (size_t)12 * r->R * r->R * 4;
+    bool staged;
+    unsigned char *dst = enc_target(Pv, out, bytes, staged);
+    GGB_CHECK(cudaMemsetAsync(dst, 0, bytes, stream()));
+    const unsigned nb = (unsigned)std::min<size_t>(((size_t)6 * r->R * r->R + 255) / 256, 148 * 8);
+    k_enc_net<<<nb, 256, 0, stream()>>>(E, reinterpret_cast<const float4 *>(r->buf), dst);
+    GGB_LAUNCHED();
+    enc_finish(Pv, out, bytes, staged);
+    return 0;
+}
+
+GGB_EXPORT int ggb_encode_preview(const Render *r, const float *bg, unsigned char *out) {
+    RenderPriv *Pv = rpriv(r);
+    EncCfg E = enc_cfg(r, Pv, bg);
+    const size_t bytes = (size_t)2 * r->R * r->R * E.ch;
+    bool staged;
+    unsigned char *dst = enc_target(Pv, out, bytes, staged);
+    const unsigned nb = (unsigned)std::min<size_t>(((size_t)2 * r->R * r->R + 255) / 256, 148 * 8);
+    k_enc_preview<<<nb, 256, 0, stream()>>>(E, reinterpret_cast<const float4 *>(r->buf), dst);
+    GGB_LAUNCHED();
+    enc_finish(Pv, out, bytes, staged);
+    return 0;
 }

@@ -51,9 +51,23 @@ int ggb_solve_trace(unsigned long long *out, int cap);
  * them) into out[6*R*R*4], host or device memory, with one device copy. */
 void ggb_render_read(const Render *r, float *out);
 
-/* Diagnostics of the last render_deposit: number of texel tiles, tiles that
- * took the sorted fallback path, and (particle, tile) list entries. */
+/* Diagnostics of the last render_deposit: number of 16x16 texel tiles, tiles
+ * composited in several key-range windows, and the record slots reserved for
+ * (sample, tile) records. */
 void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, unsigned *entries);
+
+/* The application driver's 8-bit output images (its write_outputs), encoded
+ * on the GPU from the face buffer: render_texel then render_pixel8 per texel.
+ * bg == NULL: transparent RGBA (4 channels), else RGB over bg[3] (3 channels).
+ * out is host or device memory; returns 0, or -1 with a message.
+ *  ggb_encode_faces:   6 images of R x R x ch, image k is face face_order[k]
+ *                      (NULL: 0..5; the driver's GL layout is {1,3,4,5,0,2});
+ *  ggb_encode_net:     the 4R x 3R RGBA cross net (cells without a face are 0);
+ *  ggb_encode_preview: the 2R x R x ch equirectangular preview (render_sample_dir
+ *                      at each pixel centre's longitude and latitude). */
+int ggb_encode_faces(const Render *r, const float *bg, const int *face_order, unsigned char *out);
+int ggb_encode_net(const Render *r, const float *bg, unsigned char *out);
+int ggb_encode_preview(const Render *r, const float *bg, unsigned char *out);
 
 /* cs_cell_of / cs_taps for n directions (dirs: n*3 doubles) on the GPU;
  * out: n ints; idx: n*4 ints, wt: n*4 doubles (host or device memory). */
@@ -73,6 +87,18 @@ void ggb_taps_batch(const CubeSphere *cs, const double *dirs, int n, int *idx, d
  * first call before any stream capture.  All calls share the array, so calls
  * whose GPU work overlaps (from several host threads) race. */
 int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f);
+
+/* Checkpoint / resume of a running planet.  save writes the state the next
+ * steps read (omega, omega_band, psi, vel and the last solve's statistics; the
+ * particles' pos, prev, col; the face buffer, g and a deferred fade
+ * renormalisation) to `path`; P and r may be NULL.  load restores it into
+ * objects initialised by fluid_init / particles_init / render_init with the
+ * same grid, particle count and face resolution (checked; the fluid
+ * parameters of F are kept), after which stepping continues bit-identically.
+ * Both return 0, or -1 with a message (and leave the objects' state undefined
+ * when a load fails part-way). */
+int ggb_checkpoint_save(const char *path, const Fluid *F, const Particles *P, const Render *r);
+int ggb_checkpoint_load(const char *path, Fluid *F, Particles *P, Render *r);
 
 /* Initial-condition parameters of the application driver (bands and curl noise). */
 typedef struct {

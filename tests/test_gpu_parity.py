@@ -306,6 +306,142 @@ def test_render_read_back_api(gpu, orc32):
         assert np.max(np.abs(x.astype(np.float64) - y)) <= (1 if x.dtype == np.uint8 else 1e-6)
 
 
+def _u8(a):
+    return a.ctypes.data_as(C.POINTER(C.c_ubyte))
+
+
+def _oracle_pixel(api, sp, f, x, y, bg):
+    tex = np.zeros(4, api.np_real)
+    api.lib.render_texel(C.byref(sp.r), f, x, y, api.ptr(tex))
+    px = np.array([0, 0, 0, 255], np.uint8)
+    bgv = None if bg is None else np.asarray(bg, api.np_real)
+    api.lib.render_pixel8(api.ptr(tex), None if bg is None else api.ptr(bgv), _u8(px))
+    return px
+
+
+@pytest.mark.parametrize("pending", [False, True])
+def test_encode_outputs(gpu, orc32, pending):
+    """ggb_encode_faces / _net / _preview against render_texel + render_pixel8
+    (and render_sample_dir for the preview) of the restatement; `pending`
+    leaves a fade renormalisation pending at encode time."""
+    R = 24
+    prev, pos, col = K.random_arcs(4000, seed=21, max_angle=0.08)
+    sps = {}
+    for name, api in (("gpu", gpu), ("orc", orc32)):
+        ps = G.ParticleSet(api, len(prev))
+        ps.array("prev", 3)[:] = prev
+        ps.array("pos", 3)[:] = pos
+        ps.array("col", 4)[:] = col
+        sp = G.Splat(api, R)
+        for _ in range(3):
+            sp.fade(0.02)
+        sp.deposit(ps)
+        for _ in range(460 if pending else 2):
+            sp.fade(0.02)
+        sps[name] = (sp, ps)
+    sp, osp = sps["gpu"][0], sps["orc"][0]
+    order = np.array([1, 3, 4, 5, 0, 2], np.int32)
+    for bg in (None, [0.1, 0.25, 0.5]):
+        ch = 4 if bg is None else 3
+        bgp = None if bg is None else np.asarray(bg, np.float32).ctypes.data_as(C.POINTER(C.c_float))
+        faces = np.zeros((6, R, R, ch), np.uint8)
+        assert gpu.lib.ggb_encode_faces(C.byref(sp.r), bgp, order.ctypes.data_as(C.POINTER(C.c_int)),
+                                        _u8(faces)) == 0
+        want = np.array([[[_oracle_pixel(orc32, osp, int(f), x, y, bg)[:ch] for x in range(R)] for y in range(R)]
+                         for f in order])
+        assert np.array_equal(faces, want)
+        net = np.zeros((3 * R, 4 * R, 4), np.uint8)
+        assert gpu.lib.ggb_encode_net(C.byref(sp.r), bgp, _u8(net)) == 0
+        cells = {0: (0, 1), 1: (1, 1), 2: (2, 1), 3: (3, 1), 4: (0, 0), 5: (0, 2)}
+        want_net = np.zeros_like(net)
+        for f, (cx, cy) in cells.items():
+            for y in range(R):
+                for x in range(R):
+                    px = _oracle_pixel(orc32, osp, f, x, y, bg)
+                    want_net[cy * R + y, cx * R + x] = px
+        assert np.array_equal(net, want_net)
+        prv = np.zeros((R, 2 * R, ch), np.uint8)
+        assert gpu.lib.ggb_encode_preview(C.byref(sp.r), bgp, _u8(prv)) == 0
+        want_prv = np.zeros_like(prv)
+        tex = np.zeros(4, np.float32)
+        for y in range(R):
+            lat = np.pi / 2 - (y + 0.5) / R * np.pi
+            for x in range(2 * R):
+                lon = (x + 0.5) / (2 * R) * 2 * np.pi - np.pi
+                d = (np.cos(lat) * np.sin(lon), np.sin(lat), np.cos(lat) * np.cos(lon))
+                orc32.lib.render_sample_dir(C.byref(osp.r), *d, orc32.ptr(tex))
+                px = np.array([0, 0, 0, 255], np.uint8)
+                bgv = None if bg is None else np.asarray(bg, np.float32)
+                orc32.lib.render_pixel8(orc32.ptr(tex), None if bg is None else orc32.ptr(bgv), _u8(px))
+                want_prv[y, x] = px[:ch]
+        diff = np.abs(prv.astype(int) - want_prv.astype(int))
+        # sin / cos of the two builds may differ by an ulp: a pixel may round the other way
+        assert diff.max() <= 1 and np.mean(diff > 0) < 0.01
+    for name in sps:
+        sps[name][0].free()
+        sps[name][1].free()
+
+
+def test_checkpoint_resume(gpu, tmp_path):
+    """ggb_checkpoint_save after 3 steps, 3 more steps; ggb_checkpoint_load of
+    that file into freshly initialised objects and the same 3 steps give the
+    same state bit for bit (forcing and rotation on, a fade renormalisation
+    pending at the save)."""
+    N, npart, R = 32, 3000, 32
+    g0 = gpu.grid(N)
+    vel0, vb0 = K.initial_velocity(gpu, g0)
+    g0.free()
+
+    def make():
+        g = gpu.grid(N)
+        fs = G.FluidSim(gpu, g, forcing=0.5, rotation=3.0, cg_tol=1e-6)
+        fs.set_state(vel0, vb0)
+        ps = G.ParticleSet(gpu, npart)
+        ps.colour(__import__("ggb_inputs").strip(2))
+        sp = G.Splat(gpu, R)
+        return g, fs, ps, sp
+
+    def step(g, fs, ps, sp, fade=0.02):
+        vmax = fs.max_speed()
+        dt = g.cs.h / (vmax if vmax > 1e-6 else 1e-6)
+        ps.advect(g, fs.F.vel, dt)
+        fs.step(dt)
+        sp.fade(fade)
+        sp.deposit(ps)
+
+    def state(g, fs, ps, sp):
+        return dict(omega=fs.field("omega").copy(), psi=fs.field("psi").copy(), vel=fs.field("vel", 3).copy(),
+                    pos=ps.array("pos", 3).copy(), prev=ps.array("prev", 3).copy(), faces=sp.faces(),
+                    g=float(sp.r.g), it=int(fs.F.cg_iters))
+
+    path = str(tmp_path / "planet.ckpt").encode()
+    a = make()
+    for _ in range(3):
+        step(*a)
+    for _ in range(460):  # g falls below 1e-4: a renormalisation is pending at the save
+        a[3].fade(0.02)
+    assert gpu.lib.ggb_checkpoint_save(path, C.byref(a[1].F), C.byref(a[2].P), C.byref(a[3].r)) == 0
+    for _ in range(3):
+        step(*a)
+    want = state(*a)
+    b = make()
+    assert gpu.lib.ggb_checkpoint_load(path, C.byref(b[1].F), C.byref(b[2].P), C.byref(b[3].r)) == 0
+    for _ in range(3):
+        step(*b)
+    got = state(*b)
+    for k in want:
+        assert np.array_equal(np.asarray(got[k]), np.asarray(want[k])), k
+    # a mismatched object is refused
+    c = G.ParticleSet(gpu, npart + 1)
+    assert gpu.lib.ggb_checkpoint_load(path, C.byref(b[1].F), C.byref(c.P), C.byref(b[3].r)) == -1
+    c.free()
+    for obj in (a, b):
+        obj[3].free()
+        obj[2].free()
+        obj[1].free()
+        obj[0].free()
+
+
 # -------------------------------------------------------------- particles
 
 def test_particles_init_and_colour(gpu, orc32):
