@@ -216,8 +216,8 @@ __device__ __forceinline__ D3 sample_vec(const GridDev &g, const float *fld3, D3
 // false, and every later barrier returns false at once, so a kernel can never
 // spin forever.
 struct GridBarrier {
-    unsigned int count;
-    unsigned int gen;
+    unsigned int count;  // arrivals since the launch began (zeroed by the host before each launch)
+    unsigned int gen;    // unused
     int err;
     int pad;
 };
@@ -245,37 +245,37 @@ __device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, un
     return old;
 }
 
-// Returns true when all blocks arrived; false on timeout or an earlier error.
-// Arrival is an acq_rel atomic of thread 0 after a block barrier (so every
-// write of the block before the barrier is released); the last block resets
-// the counter and releases the generation; the others poll it with acquire
-// loads.  The timeout is checked every 64 polls.
+// Returns true when all blocks arrived; false on timeout or an error raised
+// by another block.  `count` counts arrivals since the launch began (the host
+// zeroes it before every launch): thread 0 arrives with one acq_rel atomic
+// after a block barrier (so every write of the block before the barrier is
+// released), and the barrier is complete when the count reaches the next
+// multiple of the number of blocks, which the waiters poll with acquire loads.
+// The arrival is the first global access of a barrier (no generation or error
+// read before it); the error flag and the timeout are checked every 64 polls.
 __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int ok = ld_volatile_i32(&bar->err) == 0;
-        if (ok) {
-            unsigned int g = ld_acquire_u32(&bar->gen);
-            unsigned int arrived = atom_add_acq_rel_u32(&bar->count, 1u);
-            if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
-                bar->count = 0;
-                st_release_u32(&bar->gen, g + 1);
-            } else {
-                unsigned long long t0 = globaltimer_ns();
-                unsigned int polls = 0;
-                while (ld_acquire_u32(&bar->gen) == g) {
-                    if ((++polls & 63u) == 0) {
-                        if (ld_volatile_i32(&bar->err) != 0) {
-                            ok = 0;
-                            break;
-                        }
-                        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-                            atomicExch(&bar->err, 1);
-                            ok = 0;
-                            break;
-                        }
-                    }
+        const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned int old = atom_add_acq_rel_u32(&bar->count, 1u);
+        const unsigned int target = (old / nb + 1u) * nb;
+        int ok = 1;
+        unsigned long long t0 = 0;
+        unsigned int polls = 0;
+        while ((int)(ld_acquire_u32(&bar->count) - target) < 0) {
+            if ((++polls & 63u) == 0) {
+                if (ld_volatile_i32(&bar->err) != 0) {
+                    ok = 0;
+                    break;
+                }
+                const unsigned long long t = globaltimer_ns();
+                if (polls == 64u) {
+                    t0 = t;
+                } else if (t - t0 > kBarrierTimeoutNs) {
+                    atomicExch(&bar->err, 1);
+                    ok = 0;
+                    break;
                 }
             }
         }

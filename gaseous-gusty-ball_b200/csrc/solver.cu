@@ -969,6 +969,7 @@ void pcg_launch(const SolveParams &prm, cudaStream_t s) {
     SolveParams p = prm;
     size_t smem = pcg_smem_bytes(p);
     void *args[] = {&p};
+    GGB_CHECK(cudaMemsetAsync(&p.bar->count, 0, sizeof(unsigned int), s));
     GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(pcg_grid_for(smem)), dim3(kPB), args, smem, s));
     GGB_LAUNCHED();
 }
