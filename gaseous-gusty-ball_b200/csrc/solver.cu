@@ -210,6 +210,7 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
                 oc[k2 - s0] = o2.c;
             }
         }
+        stage_mark(4);
         // off-face links of each ring cell: all present neighbour values
         // requested at once, summed in link order
         for (int q = tid; q < nr; q += bs) {
@@ -1077,8 +1078,9 @@ GGB_EXPORT int ggb_solve_trace(unsigned long long *out, int cap) {
     return n;
 }
 
-// Diagnostics: enable = 1 makes block 0 of the next solves stamp the start,
-// staged and computed points of every staged phase (mark, ns); enable = 2 makes
+// Diagnostics: enable = 1 makes block 0 of the next solves stamp the start
+// (mark 1), window loaded (4), staged (2) and computed (3) points of every
+// staged phase (mark, ns); enable = 2 makes
 // every block stamp them (mark | block << 16, ns); enable = 0 stops and copies
 // out up to cap records, returning their number.
 GGB_EXPORT int ggb_stage_trace(int enable, unsigned long long *out, int cap) {
