@@ -17,7 +17,7 @@ int pcg_grid_size();
 int pcg_max_blocks();
 int pcg_max_grid_n();
 int pcg_block_size();
-void pcg_launch(const SolveParams &prm, cudaStream_t s);
+void pcg_launch(const SolveParams &prm, cudaStream_t s, int max_blocks = 0);
 int pcg_check_structured(const LevelDev &F, const LevelDev &C);
 float *pcg_build_rw16(const LevelDev &F, const LevelDev &C);
 double *pcg_dense_map(const SolveParams &prm, int l0);
@@ -113,12 +113,22 @@ __global__ void k_max_speed2(int n, const float *vel, unsigned int *out) {
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
+// The application driver's CFL step on the device (upstream src/main.c:422-426):
+// dt = cfl h / max(vmax, 1e-6), vmax the square root of k_max_speed2's maximum.
+__global__ void k_cfl_dt(const unsigned int *vmax_bits, double cfl, double h, double *dt) {
+    const double vmax = sqrt((double)__uint_as_float(*vmax_bits));
+    *dt = cfl * h / (vmax > 1e-6 ? vmax : 1e-6);
+}
+
 // ------------------------------------------------------------ advection
 
 // Midpoint backtraces (backward and, for BFECC, forward) and q0 = omega + 2 Omega y.
 // upstream src/fluid.c:397-414, 435-437
-__global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt,
-                             double two_omega, int forward, float *dep_b, float *dep_f, float *q0) {
+// dt: the time step, or *dtp when dtp is not null (a device-side CFL step).
+__global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt_in,
+                             const double *dtp, double two_omega, int forward, float *dep_b, float *dep_f,
+                             float *q0) {
+    const double dt = dtp ? *dtp : dt_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
         D3 p = load3(pos + 3 * i), u = load3(vel + 3 * i);
         D3 pm = sphere_move(p, u, -0.5 * dt);
@@ -149,9 +159,11 @@ __global__ void k_resample(GridDev g, const float *src, const float *dep, const 
 // Limited resample of the corrected source at dep_b (clamped to the range of
 // q0 over the same taps), then back to relative vorticity and relaxation
 // toward the band state.  upstream src/fluid.c:449-474
+// relax: the relaxation factor, or 1 - exp(-forcing *dtp) when dtp is not null.
 __global__ void k_limit_relax(GridDev g, const float *pos, const float *dep_b, const float *q0, const float *q2,
-                              int bfecc, double two_omega, double relax, const float *omega_band, float *q1,
-                              float *omega) {
+                              int bfecc, double two_omega, double relax_in, const double *dtp, double forcing,
+                              const float *omega_band, float *q1, float *omega) {
+    const double relax = dtp ? (forcing > 0 ? 1.0 - exp(-forcing * *dtp) : 0.0) : relax_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
         float qn;
         if (bfecc) {
@@ -427,21 +439,31 @@ static void finish_levels(Fluid *F, FluidPriv *Pv) {
 void solve_trace_target(unsigned long long **buf, int *cap);
 
 // Launch the solve and read back its result into F (sync).
-static int run_solve(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
+// Queues a solve (at most max_blocks blocks when > 0) and the copy of its
+// result; solve_collect reads the result after a synchronisation.
+static void solve_launch(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit, int max_blocks) {
     SolveParams P = solve_params(F, Pv, remove_mean, maxit);
     solve_trace_target(&P.trace, &P.trace_cap);
     cudaStream_t s = stream();
     stage_begin(ST_SOLVE);
-    pcg_launch(P, s);
+    pcg_launch(P, s, max_blocks);
     stage_end(ST_SOLVE);
     GGB_CHECK(cudaMemcpyAsync(Pv->res_host, Pv->res, sizeof(SolveResult), cudaMemcpyDeviceToHost, s));
-    GGB_CHECK(cudaStreamSynchronize(s));
-    stage_collect();
+}
+
+static int solve_collect(Fluid *F, FluidPriv *Pv) {
     const SolveResult &R = *Pv->res_host;
     if (R.status != 0) fail_msg("Poisson solve aborted: a grid barrier timed out");
     F->cg_iters = R.iters;
     F->cg_relres = R.relres;
     return R.iters;
+}
+
+static int run_solve(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit) {
+    solve_launch(F, Pv, remove_mean, maxit, 0);
+    GGB_CHECK(cudaStreamSynchronize(stream()));
+    stage_collect();
+    return solve_collect(F, Pv);
 }
 
 }  // namespace ggb
@@ -618,8 +640,9 @@ GGB_EXPORT void fluid_set_state(Fluid *F, const float *vel_initial, const float 
 }
 
 // upstream src/fluid.c:424-478
-GGB_EXPORT void fluid_step(Fluid *F, double dt) {
-    FluidPriv *Pv = priv_of(F);
+// The body of fluid_step without its synchronisation (dt, or *dtp on the
+// device when dtp is not null; the solve on at most max_blocks blocks when > 0).
+static void step_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp, int max_blocks) {
     const GridTables *t = Pv->grid0;
     cudaStream_t s = stream();
     double two_omega = 2.0 * F->prm.rotation;
@@ -627,7 +650,8 @@ GGB_EXPORT void fluid_step(Fluid *F, double dt) {
     GridDev g = t->dev();
     unsigned nb = blocks_for(t->n);
     stage_begin(ST_ADVECT);
-    k_departures<<<nb, kB, 0, s>>>(g, t->pos, F->vel, F->omega, dt, two_omega, bfecc, F->dep_b, F->dep_f, F->q0);
+    k_departures<<<nb, kB, 0, s>>>(g, t->pos, F->vel, F->omega, dt, dtp, two_omega, bfecc, F->dep_b, F->dep_f,
+                                   F->q0);
     GGB_LAUNCHED();
     k_resample<<<nb, kB, 0, s>>>(g, F->q0, F->dep_b, F->q0, 0, F->q1);
     GGB_LAUNCHED();
@@ -636,14 +660,43 @@ GGB_EXPORT void fluid_step(Fluid *F, double dt) {
         GGB_LAUNCHED();
     }
     double relax = F->prm.forcing > 0 ? 1.0 - exp(-F->prm.forcing * dt) : 0.0;
-    k_limit_relax<<<nb, kB, 0, s>>>(g, t->pos, F->dep_b, F->q0, F->q2, bfecc, two_omega, relax, F->omega_band, F->q1,
-                                    F->omega);
+    k_limit_relax<<<nb, kB, 0, s>>>(g, t->pos, F->dep_b, F->q0, F->q2, bfecc, two_omega, relax, dtp, F->prm.forcing,
+                                    F->omega_band, F->q1, F->omega);
     GGB_LAUNCHED();
     stage_end(ST_ADVECT);
-    run_solve(F, Pv, 1, F->prm.cg_maxit);
+    solve_launch(F, Pv, 1, F->prm.cg_maxit, max_blocks);
     launch_velocity(F, Pv);
-    sync();
 }
+
+GGB_EXPORT void fluid_step(Fluid *F, double dt) {
+    FluidPriv *Pv = priv_of(F);
+    step_launch(F, Pv, dt, nullptr, 0);
+    sync();
+    solve_collect(F, Pv);
+}
+
+// ---- the batched step's pieces (no synchronisation; see batch.cu) --------
+namespace ggb {
+
+// dt_dev = the driver's CFL step from the current velocity, on the device.
+void fluid_cfl_dt_launch(const Fluid *F, double cfl, double *dt_dev) {
+    FluidPriv *Pv = priv_of(F);
+    cudaStream_t s = stream();
+    const int n = F->cs->ncells;
+    GGB_CHECK(cudaMemsetAsync(Pv->vmax_bits, 0, sizeof(unsigned int), s));
+    k_max_speed2<<<blocks_for(n), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
+    GGB_LAUNCHED();
+    k_cfl_dt<<<1, 1, 0, s>>>(Pv->vmax_bits, cfl, F->cs->h, dt_dev);
+    GGB_LAUNCHED();
+}
+
+void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks) {
+    step_launch(F, priv_of(F), 0.0, dt_dev, max_blocks);
+}
+
+void fluid_step_collect(Fluid *F) { solve_collect(F, priv_of(F)); }
+
+}  // namespace ggb
 
 GGB_EXPORT double fluid_max_speed(const Fluid *F) {
     FluidPriv *Pv = priv_of(F);

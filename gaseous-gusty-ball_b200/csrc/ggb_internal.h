@@ -53,6 +53,16 @@ void stage_begin(int s);
 void stage_end(int s);
 void stage_collect();  // after a stream sync: accumulate the recorded intervals
 
+// Pieces of the batched step (batch.cu): every *_queue / *_launch call only
+// queues work on stream(); the *_collect calls run after that stream has been
+// synchronised.  dt_dev points at a device-side time step.
+void fluid_cfl_dt_launch(const Fluid *F, double cfl, double *dt_dev);
+void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks);
+void fluid_step_collect(Fluid *F);
+void render_deposit_queue(Render *r, const Particles *P);
+void render_deposit_collect(Render *r, const Particles *P);
+void particles_advect_queue(Particles *P, const CubeSphere *cs, const float *vel, const double *dt_dev);
+
 // The deferred renormalisation of render_fade (private state of a Render).
 void render_pending_get(const Render *r, int *pending, float *scale);
 void render_pending_set(Render *r, int pending, float scale);

@@ -58,7 +58,9 @@ __global__ void k_colour(int n, const float *pos, const float *img, int w, int h
 }
 
 // RK2 midpoint step; upstream src/particles.c:63-74
-__global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *vel, double dt, float *pos, float *prev) {
+__global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *vel, double dt_in, const double *dtp,
+                                                float *pos, float *prev) {
+    const double dt = dtp ? *dtp : dt_in;  // *dtp: a device-side CFL step
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float *pp = pos + 3 * (size_t)i;
         float p0 = pp[0], p1 = pp[1], p2 = pp[2];
@@ -74,12 +76,18 @@ __global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *v
     }
 }
 
-void particles_advect_launch(int n, const GridDev &g, const float *vel, double dt, float *pos, float *prev,
-                             cudaStream_t s) {
+void particles_advect_launch(int n, const GridDev &g, const float *vel, double dt, const double *dtp, float *pos,
+                             float *prev, cudaStream_t s) {
     stage_begin(ST_PARTICLES);
-    k_advect<<<blocks_for(n), kPB, 0, s>>>(n, g, vel, dt, pos, prev);
+    k_advect<<<blocks_for(n), kPB, 0, s>>>(n, g, vel, dt, dtp, pos, prev);
     GGB_LAUNCHED();
     stage_end(ST_PARTICLES);
+}
+
+void particles_advect_queue(Particles *P, const CubeSphere *cs, const float *vel, const double *dt_dev) {
+    if (P->n <= 0) return;
+    GridTables *t = grid_lookup(cs);
+    particles_advect_launch(P->n, t->dev(), vel, 0.0, dt_dev, P->pos, P->prev, stream());
 }
 
 }  // namespace ggb
@@ -130,6 +138,6 @@ GGB_EXPORT void particles_advect(Particles *P, const CubeSphere *cs, const float
     GridTables *t = grid_lookup(cs);
     Staged in;
     stage_in(in, vel, sizeof(float) * 3 * t->n);
-    particles_advect_launch(P->n, t->dev(), (const float *)in.dev, dt, P->pos, P->prev, stream());
+    particles_advect_launch(P->n, t->dev(), (const float *)in.dev, dt, nullptr, P->pos, P->prev, stream());
     sync();
 }

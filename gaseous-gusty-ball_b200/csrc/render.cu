@@ -42,6 +42,14 @@ struct __align__(16) Rec {
     float4 col;
 };
 
+struct SplatCfg {
+    int R, ntx, ntiles;
+    float rad, invrad, invg, alpha;
+    double spacing;
+    int renorm;
+    float scale;
+};
+
 struct RenderPriv {
     int R = 0, ntx = 0, ntiles = 0;
     unsigned *tile_count = nullptr, *tile_start = nullptr, *tile_fill = nullptr;
@@ -51,6 +59,7 @@ struct RenderPriv {
     unsigned *total_host = nullptr;  // pinned: [0] reserved record slots, [1] slot overflow
     bool pending = false;
     float pending_scale = 1.f;
+    SplatCfg queued{};             // configuration of the last queued deposit (for its repeat)
     float *mirror = nullptr;
     unsigned char *enc = nullptr;  // device scratch of the 8-bit encoders (host outputs)
     size_t enc_cap = 0;
@@ -63,13 +72,6 @@ static RenderPriv *rpriv(const Render *r) {
     return reinterpret_cast<RenderPriv *>(r->tr);
 }
 
-struct SplatCfg {
-    int R, ntx, ntiles;
-    float rad, invrad, invg, alpha;
-    double spacing;
-    int renorm;
-    float scale;
-};
 
 // Sample k of the arc a -> b (chord lerp, normalised), FP64 with the
 // contraction pattern of the upstream build.
@@ -794,10 +796,12 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
     stage_end(ST_TILES);
 }
 
-// The whole deposit without a host round trip; returns after queueing it.
-// render_deposit checks, after its synchronisation, that the record buffer was
-// large enough, and otherwise grows it and repeats the fill and composite.
-void render_deposit_launch(Render *r, const Particles *P) {
+// The whole deposit without a host round trip: queues count, scan, fill and
+// compositing and the copies of the reserved total and the overflow flag.
+// render_deposit_collect (after a synchronisation of the stream) checks that
+// the record buffer was large enough and otherwise grows it and repeats the
+// fill and compositing (which skipped: the face buffer is untouched).
+void render_deposit_queue(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
@@ -817,7 +821,14 @@ void render_deposit_launch(Render *r, const Particles *P) {
     deposit_fill_tiles(r, P, Pv, C);
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    GGB_CHECK(cudaStreamSynchronize(s));
+    Pv->queued = C;
+    Pv->pending = false;
+    Pv->pending_scale = 1.f;
+    Pv->dev_gen++;
+}
+
+void render_deposit_collect(Render *r, const Particles *P) {
+    RenderPriv *Pv = rpriv(r);
     if (Pv->total_host[1])
         fail_msg("render_deposit: a tile's sample records exceeded the slots reserved for them (internal error)");
     const size_t need = Pv->total_host[0];
@@ -825,12 +836,17 @@ void render_deposit_launch(Render *r, const Particles *P) {
         dev_free(Pv->recs);
         Pv->rec_cap = need + need / 4 + 1024;
         Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
-        GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
-        deposit_fill_tiles(r, P, Pv, C);
+        GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, stream()));
+        deposit_fill_tiles(r, P, Pv, Pv->queued);
+        GGB_CHECK(cudaStreamSynchronize(stream()));
+        Pv->dev_gen++;
     }
-    Pv->pending = false;
-    Pv->pending_scale = 1.f;
-    Pv->dev_gen++;
+}
+
+void render_deposit_launch(Render *r, const Particles *P) {
+    render_deposit_queue(r, P);
+    GGB_CHECK(cudaStreamSynchronize(stream()));
+    render_deposit_collect(r, P);
 }
 
 static void refresh_mirror(const Render *r, RenderPriv *Pv) {

@@ -966,12 +966,16 @@ static int pcg_grid_for(size_t smem) {
 
 int pcg_grid_size() { return pcg_grid_for(kStageBytes); }
 
-void pcg_launch(const SolveParams &prm, cudaStream_t s) {
+// One solve launch; max_blocks > 0 caps its grid (batched planets: small
+// grids take a share of the SMs so that several solves run at once).
+void pcg_launch(const SolveParams &prm, cudaStream_t s, int max_blocks) {
     SolveParams p = prm;
     size_t smem = pcg_smem_bytes(p);
     void *args[] = {&p};
+    int grid = pcg_grid_for(smem);
+    if (max_blocks > 0) grid = std::max(1, std::min(grid, max_blocks));
     GGB_CHECK(cudaMemsetAsync(&p.bar->count, 0, sizeof(unsigned int), s));
-    GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(pcg_grid_for(smem)), dim3(kPB), args, smem, s));
+    GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPB), args, smem, s));
     GGB_LAUNCHED();
 }
 

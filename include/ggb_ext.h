@@ -100,6 +100,28 @@ int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f);
 int ggb_checkpoint_save(const char *path, const Fluid *F, const Particles *P, const Render *r);
 int ggb_checkpoint_load(const char *path, Fluid *F, Particles *P, Render *r);
 
+/* Batched planets.  A planet is the usual objects (cs_init, fluid_init,
+ * particles_init, render_init; planets of the same N may share a grid).
+ * ggb_batch_step advances every planet by `steps` application-driver steps
+ * (CFL dt from the maximum speed, particles_advect, fluid_step, render_fade,
+ * render_deposit), queueing each planet's work on its own stream with the
+ * CFL dt computed on the device, so that the planets' kernels overlap and
+ * nothing returns to the host inside a step; it synchronises once per step.
+ * A planet's solve runs on one block per `cells_per_block` cells (default
+ * 2048, at most one per SM), so small planets solve side by side.  P[i] and
+ * r[i] may be NULL (fluid only); fade[i] is render_fade's argument.
+ * Results equal the per-planet entry points' up to the order of the solve's
+ * FP64 block sums (a different grid) and the device's exp in the forcing's
+ * relaxation factor.  create returns NULL with a message on bad arguments;
+ * step returns 0. */
+typedef struct GGBBatch GGBBatch;
+GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *P, Render *const *r, const double *cfl,
+                           const double *fade);
+int ggb_batch_step(GGBBatch *b, int steps);
+int ggb_batch_cells_per_block(GGBBatch *b, int cells); /* cells <= 0: query */
+void ggb_batch_dt(const GGBBatch *b, double *dt);      /* the last step's dt per planet */
+void ggb_batch_free(GGBBatch *b);
+
 /* Initial-condition parameters of the application driver (bands and curl noise). */
 typedef struct {
 	int bands;

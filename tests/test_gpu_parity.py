@@ -503,3 +503,80 @@ def test_host_pointer_operands(gpu, orc32):
     n0 = gpu.lib.ggb_launch_count()
     K.operators(gpu, 16)
     assert gpu.lib.ggb_launch_count() > n0
+
+
+# ---------------------------------------------------------------- batched planets
+
+def _batch_planets(api, specs, forcing, rotation):
+    """specs: (N, particles, R, seed) per planet."""
+    out = []
+    for N, npart, R, seed in specs:
+        g = api.grid(N)
+        vel, vb = K.initial_velocity(api, g, seed=seed)
+        fs = G.FluidSim(api, g, forcing=forcing, rotation=rotation, cg_tol=1e-6)
+        fs.set_state(vel, vb if forcing > 0 else None)
+        ps = G.ParticleSet(api, npart)
+        ps.colour(__import__("ggb_inputs").strip(seed))
+        sp = G.Splat(api, R)
+        out.append((g, fs, ps, sp))
+    return out
+
+
+def _batch_state(pl):
+    g, fs, ps, sp = pl
+    return dict(omega=fs.field("omega").copy(), psi=fs.field("psi").copy(), vel=fs.field("vel", 3).copy(),
+                pos=ps.array("pos", 3).copy(), faces=sp.faces(), g=float(sp.r.g), it=int(fs.F.cg_iters))
+
+
+def _batch_free(pls):
+    for g, fs, ps, sp in pls:
+        sp.free()
+        ps.free()
+        fs.free()
+        g.free()
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_batched_step_matches_per_planet(gpu, exact):
+    """ggb_batch_step against the per-planet entry points (the driver's step
+    with dt = cfl h / vmax).  exact: one solve block per SM and no forcing,
+    so the batched arithmetic is the per-planet arithmetic, bit for bit;
+    otherwise small per-planet solve grids and forcing, within 1e-5."""
+    specs = [(16, 1500, 32, 3), (32, 3000, 40, 4), (24, 2000, 32, 5)]
+    forcing, rotation = (0.0, 2.0) if exact else (0.5, 2.0)
+    steps, cfl, fade = 3, 1.0, 0.02
+    ref = _batch_planets(gpu, specs, forcing, rotation)
+    for _ in range(steps):
+        for g, fs, ps, sp in ref:
+            vmax = fs.max_speed()
+            dt = cfl * g.cs.h / (vmax if vmax > 1e-6 else 1e-6)
+            ps.advect(g, fs.F.vel, dt)
+            fs.step(dt)
+            sp.fade(fade)
+            sp.deposit(ps)
+    want = [_batch_state(pl) for pl in ref]
+    _batch_free(ref)
+    bat = _batch_planets(gpu, specs, forcing, rotation)
+    n = len(bat)
+    T = gpu.T
+    Fs = (C.POINTER(T["Fluid"]) * n)(*[C.pointer(pl[1].F) for pl in bat])
+    Ps = (C.POINTER(T["Particles"]) * n)(*[C.pointer(pl[2].P) for pl in bat])
+    Rs = (C.POINTER(T["Render"]) * n)(*[C.pointer(pl[3].r) for pl in bat])
+    cf = (C.c_double * n)(*([cfl] * n))
+    fd = (C.c_double * n)(*([fade] * n))
+    b = gpu.lib.ggb_batch_create(n, Fs, Ps, Rs, cf, fd)
+    assert b
+    if exact:
+        gpu.lib.ggb_batch_cells_per_block(b, 1)
+    assert gpu.lib.ggb_batch_step(b, steps) == 0
+    got = [_batch_state(pl) for pl in bat]
+    gpu.lib.ggb_batch_free(b)
+    _batch_free(bat)
+    for w, g_ in zip(want, got):
+        for k in ("omega", "psi", "vel", "pos", "faces"):
+            if exact:
+                assert np.array_equal(w[k], g_[k]), k
+            else:
+                assert rel_l2(g_[k], w[k]) <= 1e-5, k
+        assert w["g"] == g_["g"]
+        assert abs(w["it"] - g_["it"]) <= (0 if exact else 1)
