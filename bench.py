@@ -55,14 +55,25 @@ def args_():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["default", "batch"], default="default",
-                   help="batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping")
+    p.add_argument("--workload", choices=["default", "large", "batch"], default="default",
+                   help="large: N=512, 4M particles, 2048^2 faces, forcing 0.5, rotation 10; "
+                        "batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping")
     p.add_argument("--cells-per-block", type=int, default=0,
                    help="batch: cells per block of the batched solves (0: tune over a few candidates)")
     return p.parse_args()
 
 
 # ---------------------------------------------------------------- helpers
+
+def working_set_note(cfg):
+    """Per-step working set against the 126 MB L2 (no L2 flush between steps)."""
+    faces = 6 * cfg["R"] ** 2 * 16
+    parts = cfg["particles"] * 40
+    fluid = 6 * cfg["N"] ** 2 * 250  # fields, operator tables, hierarchy
+    tot = faces + parts + fluid
+    return (f"per-step working set ~{tot / 1e9:.2f} GB (face buffer {faces / 1e6:.0f} MB, particles "
+            f"{parts / 1e6:.0f} MB, fields and tables ~{fluid / 1e6:.0f} MB) exceeds the 126 MB L2")
+
 
 class Planet:
     """One planet (grid, fluid, particles, faces) of a library."""
@@ -320,7 +331,7 @@ def run_ours(a, rank, world, local):
     traffic = None
     try:
         tj = json.load(open(TRAFFIC))
-        if tj.get("kernel_stage") == dom:
+        if tj.get("kernel_stage") == dom and tj.get("workload", "default") == a.workload:
             traffic = tj.get("bytes_per_launch")
     except (OSError, ValueError):
         pass
@@ -335,8 +346,7 @@ def run_ours(a, rank, world, local):
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world} (one planet per GPU)",
-                       "l2": "per-step working set ~0.25 GB (face buffer 100 MB, particles 40 MB, fields and "
-                             "tables ~100 MB) exceeds the 126 MB L2",
+                       "l2": working_set_note(CFG),
                        "mean_cg_iters": kit,
                        "stage_ms_per_step": {k: v[0] / KS for k, v in per_stage.items()},
                        "stage_steps": KS},
@@ -378,12 +388,32 @@ def batch_specs(count=64, seed=7):
 
 def run_batch(a, rank, world, local):
     """64 uneven planets advanced by ggb_batch_step, against the same planets
-    stepped one after another through the per-planet entry points."""
+    stepped one after another through the per-planet entry points.  With N
+    ranks every rank takes its share of the planets (longest processing time
+    first by estimated cost, ggb_shard.assign); no collective on the data
+    path, the job time is the maximum over ranks."""
     import torch
-    api = G.Api(G.PRODUCT_LIB)
+    import ggb_shard
+    dist = None
     if world > 1:
-        api.lib.ggb_set_device(local)
-    specs = batch_specs()
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    api = G.Api(G.PRODUCT_LIB)
+    if api.lib.ggb_set_device(local) != 0:
+        raise RuntimeError(f"cannot select CUDA device {local}")
+
+    def barrier():
+        if dist:
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(x):
+        return ggb_shard.max_over_ranks(x, dist, f"cuda:{local}") if dist else float(x)
+
+    all_specs = batch_specs()
+    owned, _ = ggb_shard.assign([ggb_shard.planet_cost(p["N"], p["particles"], p["R"]) for p in all_specs], world)
+    specs = [all_specs[i] for i in owned[rank]]
     grids = {}
     planets = []
     for sp in specs:
@@ -444,35 +474,38 @@ def run_batch(a, rank, world, local):
     its = []
     half = max(1, K // 2)
     for seg in range(2):
+        barrier()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
         api.lib.ggb_batch_step(b, half)
-        ms_b += max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0))
+        ms_b += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
         its += [p[1].F.cg_iters for p in planets]
+        barrier()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
         for _ in range(half):
             for p in planets:
                 plain_step(p)
-        ms_p += max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0))
+        ms_p += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
     clocks = stop_clock_sampler(clk, clk_path)
     K = 2 * half
     api.lib.ggb_batch_free(b)
-    cells = sum(p[0].n for p in planets)
-    parts = sum(p[4]["particles"] for p in planets)
-    value = world * n * K / (ms_b / 1000.0)
-    plain = world * n * K / (ms_p / 1000.0)
+    cells = sum(6 * p["N"] ** 2 for p in all_specs)
+    parts = sum(p["particles"] for p in all_specs)
+    value = len(all_specs) * K / (ms_b / 1000.0)
+    plain = len(all_specs) * K / (ms_p / 1000.0)
     if rank == 0:
         print(json.dumps({
             "metric": "planet-steps/s (64 uneven planets, batched)", "value": value, "unit": "planet-steps/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_b / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "plain": {"value": plain, "unit": "planet-steps/s", "ms_per_step": ms_p / K,
                       "note": "the same planets, each stepped through the per-planet entry points in turn"},
             "speedup_vs_plain": value / plain,
             "config": {"workload": "64 planets, N uniform in {64,128,256}, particles uniform in [100k,1M], faces "
                                    "512^2 or 1024^2, bands in {4,8,12}, noise scale in [2,5], PCG tol 1e-6, CFL 1",
-                       "planets_by_N": {str(k): sum(1 for p in planets if p[4]["N"] == k) for k in (64, 128, 256)},
+                       "planets_by_N": {str(k): sum(1 for p in all_specs if p["N"] == k) for k in (64, 128, 256)},
+                       "parallelism": f"batch sharded over {world} GPU(s) by estimated planet cost (LPT)",
                        "cells": cells, "particles": parts, "mean_cg_iters": float(np.mean(its)),
                        "psi_error": "batched and plain run the same FP32 solve to the same tolerance",
                        "cells_per_block": best, "tuning_ms_per_step": {str(k): v for k, v in tried.items()},
@@ -484,6 +517,9 @@ def run_batch(a, rank, world, local):
         fs.free()
     for g in grids.values():
         g.free()
+    if dist:
+        barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -491,6 +527,13 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.workload == "large":
+        global CFG, METRIC, WORKLOAD
+        CFG = dict(ggb_inputs.DEFAULT, N=512, particles=4_000_000, R=2048, forcing=0.5, rotation=10.0)
+        METRIC = "steps/s (N=512, 4M particles)"
+        WORKLOAD = ("N=512 equiangular cubed sphere (1,572,864 cells), 4,000,000 particles, 6 x 2048^2 RGBA faces, "
+                    "forcing 0.5, rotation 10, multigrid-PCG to relative residual 1e-6 (FP32 storage), CFL 1, "
+                    "fade 0.02, splat radius 1, alpha 0.35, 8 bands + 4-octave curl noise (seed 1)")
     if a.impl == "reference":
         run_reference(a, rank, world)
     elif a.workload == "batch":
