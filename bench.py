@@ -489,6 +489,9 @@ def run_batch(a, rank, world, local):
         ms_p += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
     clocks = stop_clock_sampler(clk, clk_path)
     K = 2 * half
+    wq, cq = C.c_double(), C.c_double()
+    host_enq = api.lib.ggb_batch_host_ms(b, C.byref(wq), C.byref(cq))
+    host_ms = {"enqueue": host_enq, "gpu_wait": wq.value, "collect": cq.value}
     api.lib.ggb_batch_free(b)
     cells = sum(6 * p["N"] ** 2 for p in all_specs)
     parts = sum(p["particles"] for p in all_specs)
@@ -509,6 +512,7 @@ def run_batch(a, rank, world, local):
                        "cells": cells, "particles": parts, "mean_cg_iters": float(np.mean(its)),
                        "psi_error": "batched and plain run the same FP32 solve to the same tolerance",
                        "cells_per_block": best, "tuning_ms_per_step": {str(k): v for k, v in tried.items()},
+                       "host_ms_last_step": host_ms,
                        "timing": "max of CUDA events on the library stream and the host wall clock"},
             "clocks": clocks}), flush=True)
     for g, fs, ps, spl, sp in planets:

@@ -20,6 +20,7 @@
 // Results equal the per-planet entry points' up to the relaxation factor of
 // the forcing, 1 - exp(-forcing dt), which the device computes with its own
 // exp (last-bit differences).
+#include <chrono>
 #include <cstdio>
 #include <vector>
 
@@ -35,6 +36,7 @@ struct GGBBatch {
     double *dt_dev = nullptr;  // [n] device-side time steps
     int cells_per_block = 2048;
     cudaEvent_t fork = nullptr;
+    double enqueue_ms = 0, wait_ms = 0, collect_ms = 0;  // host time of the last step's three parts
 };
 
 using namespace ggb;
@@ -84,7 +86,9 @@ GGB_EXPORT void ggb_batch_dt(const GGBBatch *b, double *dt) {
 GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
     if (!b) return -1;
     const cudaStream_t base = stream();
+    using clk = std::chrono::steady_clock;
     for (int k = 0; k < steps; k++) {
+        const auto t0 = clk::now();
         // every planet's stream starts after the work already queued on the library stream
         GGB_CHECK(cudaEventRecord(b->fork, base));
         for (int i = 0; i < b->n; i++) {
@@ -100,16 +104,30 @@ GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
                 if (b->P[i]) render_deposit_queue(b->r[i], b->P[i]);
             }
         }
+        const auto t1 = clk::now();
         for (int i = 0; i < b->n; i++) GGB_CHECK(cudaStreamSynchronize(b->st[i]));
+        const auto t2 = clk::now();
         for (int i = 0; i < b->n; i++) {
             set_stream(b->st[i]);
             fluid_step_collect(b->F[i]);
             if (b->r[i] && b->P[i]) render_deposit_collect(b->r[i], b->P[i]);
         }
         set_stream(nullptr);
+        const auto t3 = clk::now();
+        b->enqueue_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        b->wait_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        b->collect_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
     }
     set_stream(nullptr);
     return 0;
+}
+
+// Diagnostics: host time (ms) of the last batched step's queueing, waiting
+// for the GPU, and collecting; returns the queueing time.
+GGB_EXPORT double ggb_batch_host_ms(const GGBBatch *b, double *wait_ms, double *collect_ms) {
+    if (wait_ms) *wait_ms = b->wait_ms;
+    if (collect_ms) *collect_ms = b->collect_ms;
+    return b->enqueue_ms;
 }
 
 GGB_EXPORT void ggb_batch_free(GGBBatch *b) {

@@ -223,7 +223,8 @@ __device__ __forceinline__ unsigned arc_samples_bound(D3 a, D3 b, double spacing
     return (unsigned)min(max((int)ceilf(q) + 1, 1), kMaxSamples);
 }
 
-__global__ void k_rd_count(int n, SplatCfg C, const float *prev, const float *pos, unsigned *tile_count) {
+__global__ void __launch_bounds__(256, 4) k_rd_count(int n, SplatCfg C, const float *prev, const float *pos,
+                                                     unsigned *tile_count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 a = load3(prev + 3 * (size_t)i), b = load3(pos + 3 * (size_t)i);
         const unsigned nsb = arc_samples_bound(a, b, C.spacing);

@@ -152,6 +152,7 @@ class Api:
             ("ggb_batch_cells_per_block", C.c_int, [C.c_void_p, C.c_int]),
             ("ggb_batch_dt", None, [C.c_void_p, P(C.c_double)]),
             ("ggb_batch_free", None, [C.c_void_p]),
+            ("ggb_batch_host_ms", C.c_double, [C.c_void_p, P(C.c_double), P(C.c_double)]),
             ("ggb_checkpoint_load", C.c_int, [C.c_char_p, P(T["Fluid"]), P(T["Particles"]), P(T["Render"])]),
             ("ggb_encode_preview", C.c_int, [P(T["Render"]), P(C.c_float), P(C.c_ubyte)]),
             ("ggb_initial_velocity", None, [P(T["CubeSphere"]), P(InitParams), R, R]),

@@ -120,6 +120,8 @@ GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *P, Render *
 int ggb_batch_step(GGBBatch *b, int steps);
 int ggb_batch_cells_per_block(GGBBatch *b, int cells); /* cells <= 0: query */
 void ggb_batch_dt(const GGBBatch *b, double *dt);      /* the last step's dt per planet */
+/* host time (ms) of the last step's queueing (returned), GPU wait and collection */
+double ggb_batch_host_ms(const GGBBatch *b, double *wait_ms, double *collect_ms);
 void ggb_batch_free(GGBBatch *b);
 
 /* Initial-condition parameters of the application driver (bands and curl noise). */
