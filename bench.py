@@ -330,10 +330,10 @@ def run_ours(a, rank, world, local):
     peak, peak_kind = measured_peak_hbm()
     traffic = None
     try:
-        tj = json.load(open(TRAFFIC))
-        if tj.get("kernel_stage") == dom and tj.get("workload", "default") == a.workload:
-            traffic = tj.get("bytes_per_launch")
-    except (OSError, ValueError):
+        for tj in json.load(open(TRAFFIC)):
+            if tj.get("kernel_stage") == dom and tj.get("workload") == a.workload:
+                traffic = tj.get("bytes_per_launch")
+    except (OSError, ValueError, AttributeError):
         pass
 
     base = None
