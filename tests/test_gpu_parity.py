@@ -155,6 +155,21 @@ def test_poisson(gpu, orc32, N, multigrid):
         assert rel_l2(a["psi"], ex) < 0.02   # upstream tests/test_poisson.c:72
 
 
+def test_poisson_N512_staged_subranges(gpu, orc64):
+    """N=512 (1,572,864 cells): every block's level-0 range (10,628 cells)
+    exceeds the staged window, so each solve phase runs in several
+    sub-ranges; against the FP64 oracle solved to 1e-10."""
+    orc64.lib.drv_set_threads(orc64.lib.drv_max_threads())
+    try:
+        b = K.poisson(orc64, 512, tol=1e-10)
+    finally:
+        orc64.lib.drv_set_threads(1)
+    a = K.poisson(gpu, 512, tol=1e-6)
+    assert a["relres"] <= 1e-6
+    assert rel_l2(a["psi"], b["psi"]) < 1e-4
+    assert rel_l2(a["vel"], b["vel"]) < 1e-4
+
+
 def test_poisson_golden(gpu):
     a, gold = K.poisson(gpu, 16), golden("poisson_N16")
     assert int(a["iters"]) == int(gold["iters"])
