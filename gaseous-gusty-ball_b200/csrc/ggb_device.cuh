@@ -217,9 +217,7 @@ __device__ __forceinline__ D3 sample_vec(const GridDev &g, const float *fld3, D3
 // spin forever.
 struct GridBarrier {
     unsigned int count;  // arrivals since the launch began (zeroed by the host before each launch)
-    unsigned int gen;    // unused
-    int err;
-    int pad;
+    int err;             // sticky: a barrier timed out
 };
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
@@ -233,9 +231,6 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
     unsigned int v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile_i32(const int *p) { return *(volatile const int *)p; }
 
