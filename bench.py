@@ -315,7 +315,8 @@ def run_ours(a, rank, world, local):
     kit = float(np.mean(its))
     per_stage = {STAGES[i]: (st_ms[i], st_n[i]) for i in range(7)}
     dom = max(per_stage, key=lambda k: per_stage[k][0])
-    # algorithmic bytes per launch (SURVEY byte model, per cell / per particle)
+    # algorithmic bytes per launch: one read of every input array and one write of every output
+    # array per pass of the upstream step (4 B scalars, 12 B vectors, 4 B per link weight)
     bytes_model = {
         "solve": n * (16 + 36 + 12 + 16 + kit * (76 + 253)),
         "advect": n * (48 + 12 + 20 + 20 + 12 + 24 + 16),

@@ -9,7 +9,8 @@ over ranks.
 
 
 def planet_cost(N, particles, R, cg_iters=8):
-    """Estimated bytes moved per step: fluid (SURVEY byte model), particles and faces."""
+    """Estimated bytes moved per step: fluid (one read of every input and one write of every
+    output per pass of the upstream step, K_it CG iterations), particles and faces."""
     n = 6 * N * N
     return n * (344 + 253 + cg_iters * (76 + 253)) + 76 * particles + 32 * 6 * R * R
 
