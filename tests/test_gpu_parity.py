@@ -595,3 +595,38 @@ def test_batched_step_matches_per_planet(gpu, exact):
                 assert rel_l2(g_[k], w[k]) <= 1e-5, k
         assert w["g"] == g_["g"]
         assert abs(w["it"] - g_["it"]) <= (0 if exact else 1)
+
+
+def test_batched_step_fluid_only_planet(gpu):
+    """A planet without particles and faces (P[i] = r[i] = NULL) in a batch:
+    its fluid state equals the per-planet entry points' bit for bit."""
+    N, steps, cfl = 24, 3, 1.0
+    g = gpu.grid(N)
+    vel, _ = K.initial_velocity(gpu, g, seed=9)
+    ref = G.FluidSim(gpu, g, rotation=1.5, cg_tol=1e-6)
+    ref.set_state(vel, None)
+    for _ in range(steps):
+        vmax = ref.max_speed()
+        ref.step(cfl * g.cs.h / (vmax if vmax > 1e-6 else 1e-6))
+    want = (ref.field("omega").copy(), ref.field("psi").copy(), ref.field("vel", 3).copy())
+    ref.free()
+    full = _batch_planets(gpu, [(16, 1000, 32, 3)], 0.0, 1.5)
+    fs = G.FluidSim(gpu, g, rotation=1.5, cg_tol=1e-6)
+    fs.set_state(vel, None)
+    T = gpu.T
+    Fs = (C.POINTER(T["Fluid"]) * 2)(C.pointer(full[0][1].F), C.pointer(fs.F))
+    Ps = (C.POINTER(T["Particles"]) * 2)(C.pointer(full[0][2].P), None)
+    Rs = (C.POINTER(T["Render"]) * 2)(C.pointer(full[0][3].r), None)
+    cf = (C.c_double * 2)(cfl, cfl)
+    fd = (C.c_double * 2)(0.02, 0.0)
+    b = gpu.lib.ggb_batch_create(2, Fs, Ps, Rs, cf, fd)
+    assert b
+    gpu.lib.ggb_batch_cells_per_block(b, 1)
+    assert gpu.lib.ggb_batch_step(b, steps) == 0
+    got = (fs.field("omega").copy(), fs.field("psi").copy(), fs.field("vel", 3).copy())
+    gpu.lib.ggb_batch_free(b)
+    fs.free()
+    g.free()
+    _batch_free(full)
+    for w, x in zip(want, got):
+        assert np.array_equal(w, x)

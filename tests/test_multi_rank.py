@@ -73,3 +73,24 @@ def test_two_gloo_ranks_agree():
     assert sorted(out[0][0] + out[1][0]) == list(range(len(costs)))
     tmax = max(out[0][1], out[1][1])
     assert out[0][2] == tmax and out[1][2] == tmax
+
+
+def test_batch_workload_is_deterministic_and_sharded():
+    """The batched workload's 64 planets (bench.batch_specs) are the same on
+    every call and rank, drawn from the stated ranges, and every planet goes
+    to exactly one rank."""
+    import importlib.util
+    root = os.path.dirname(PKG)
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    a, b = bench.batch_specs(), bench.batch_specs()
+    assert a == b and len(a) == 64
+    assert {p["N"] for p in a} <= {64, 128, 256} and {p["R"] for p in a} <= {512, 1024}
+    assert all(100_000 <= p["particles"] <= 1_000_000 and p["bands"] in (4, 8, 12) for p in a)
+    assert all(2.0 <= p["noise_scale"] <= 5.0 for p in a) and len({p["seed"] for p in a}) == 64
+    costs = [ggb_shard.planet_cost(p["N"], p["particles"], p["R"]) for p in a]
+    for world in (1, 2, 4, 8):
+        owned, loads = ggb_shard.assign(costs, world)
+        assert sorted(i for o in owned for i in o) == list(range(64))
+        assert max(loads) <= sum(costs) / world + max(costs)
