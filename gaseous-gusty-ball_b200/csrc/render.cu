@@ -55,11 +55,13 @@ struct RenderPriv {
     unsigned *tile_count = nullptr, *tile_start = nullptr, *tile_fill = nullptr;
     Rec *recs = nullptr;
     size_t rec_cap = 0;
-    unsigned *diag = nullptr;        // device: [0] windowed tiles of the last deposit, [1] slot overflow (sticky)
+    unsigned *diag = nullptr;        // device: [0] windowed tiles of the last deposit, [1] tiles whose slots overflowed
     unsigned *total_host = nullptr;  // pinned: [0] reserved record slots, [1] slot overflow
     bool pending = false;
     float pending_scale = 1.f;
     SplatCfg queued{};             // configuration of the last queued deposit (for its repeat)
+    bool queued_est = false;       // its slots were estimated from the previous deposit's fills
+    bool have_prev = false;        // tile_fill holds the previous deposit's record counts
     float *mirror = nullptr;
     unsigned char *enc = nullptr;  // device scratch of the 8-bit encoders (host outputs)
     size_t enc_cap = 0;
@@ -378,7 +380,12 @@ __global__ void k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos
 // Exclusive scan of cnt[0..n) into start[0..n] (one block of 1024 threads).
 // The counts of up to 32 chunks of 1024 are loaded at once (coalesced, one
 // memory latency), then scanned chunk after chunk with warp shuffles.
-__global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, unsigned *start, unsigned *total) {
+// est: the counts are the previous deposit's record counts, and each tile
+// reserves that count plus half of it plus 32 (records of a tile change little
+// from one step to the next; a tile that still overflows makes the deposit
+// repeat with exact reservations).
+__global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, int est, unsigned *start,
+                                                   unsigned *total) {
     constexpr int kChunks = 32;
     __shared__ unsigned s_w[32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -388,7 +395,8 @@ __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, 
 #pragma unroll
         for (int c = 0; c < kChunks; c++) {
             const int i = g0 + c * 1024 + t;
-            v[c] = i < n ? __ldg(cnt + i) : 0u;
+            const unsigned x = i < n ? cnt[i] : 0u;
+            v[c] = i < n ? (est ? x + x / 2 + 32u : x) : 0u;
         }
 #pragma unroll
         for (int c = 0; c < kChunks; c++) {
@@ -681,6 +689,7 @@ __global__ void __launch_bounds__(kTB) k_rd_tiles(SplatCfg C, const unsigned *ti
                                                   const unsigned *tile_fill, const Rec *recs, size_t cap,
                                                   float *buf, unsigned *diag) {
     if (tile_start[C.ntiles] > cap) return;  // records not filled: see k_rd_fill
+    if (diag[1]) return;                     // a tile's records overflowed: the deposit is repeated
     __shared__ TileSmem S;
     const int tile = blockIdx.x, q = threadIdx.x;
     const int R = C.R, ntx = C.ntx;
@@ -797,51 +806,97 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
     stage_end(ST_TILES);
 }
 
-// The whole deposit without a host round trip: queues count, scan, fill and
-// compositing and the copies of the reserved total and the overflow flag.
-// render_deposit_collect (after a synchronisation of the stream) checks that
-// the record buffer was large enough and otherwise grows it and repeats the
-// fill and compositing (which skipped: the face buffer is untouched).
+// The whole deposit without a host round trip: queues the slot reservation,
+// scan, fill and compositing and the copies of the reserved total and the
+// overflow count.  The reservation is exact (k_rd_count) for the first deposit
+// and estimated from the previous deposit's per-tile record counts afterwards
+// (no counting pass).  render_deposit_collect (after a synchronisation of the
+// stream) checks the outcome: when the record buffer was too small or an
+// estimated tile overflowed, fill and compositing skipped (the face buffer is
+// untouched) and the deposit is repeated with exact reservations.
 void render_deposit_queue(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
+    const bool est = Pv->have_prev;
     stage_begin(ST_BIN);
-    GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
-    GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
-    GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, sizeof(unsigned), s));
-    unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
-    if (n > 0) {
-        k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
+    GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
+    if (est) {
+        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_fill, 1, Pv->tile_start, Pv->tile_count + Pv->ntiles);
+        GGB_LAUNCHED();
+    } else {
+        GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
+        unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
+        if (n > 0) {
+            k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
+            GGB_LAUNCHED();
+        }
+        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles);
         GGB_LAUNCHED();
     }
-    k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, Pv->tile_start, Pv->tile_count + Pv->ntiles);
-    GGB_LAUNCHED();
+    GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
     stage_end(ST_BIN);
     deposit_fill_tiles(r, P, Pv, C);
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     Pv->queued = C;
+    Pv->queued_est = est;
     Pv->pending = false;
     Pv->pending_scale = 1.f;
     Pv->dev_gen++;
 }
 
-void render_deposit_collect(Render *r, const Particles *P) {
-    RenderPriv *Pv = rpriv(r);
-    if (Pv->total_host[1])
-        fail_msg("render_deposit: a tile's sample records exceeded the slots reserved for them (internal error)");
+// The queued deposit again with exact reservations (synchronous).
+static void deposit_exact(Render *r, const Particles *P, RenderPriv *Pv) {
+    cudaStream_t s = stream();
+    const SplatCfg &C = Pv->queued;
+    const int n = P->n;
+    GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
+    GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
+    unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
+    if (n > 0) {
+        k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
+        GGB_LAUNCHED();
+    }
+    k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles);
+    GGB_LAUNCHED();
+    GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaStreamSynchronize(s));
     const size_t need = Pv->total_host[0];
     if (need > Pv->rec_cap) {
         dev_free(Pv->recs);
         Pv->rec_cap = need + need / 4 + 1024;
         Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
-        GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, stream()));
-        deposit_fill_tiles(r, P, Pv, Pv->queued);
-        GGB_CHECK(cudaStreamSynchronize(stream()));
-        Pv->dev_gen++;
     }
+    GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
+    deposit_fill_tiles(r, P, Pv, C);
+    GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaStreamSynchronize(s));
+    if (Pv->total_host[1])
+        fail_msg("render_deposit: a tile's sample records exceeded their exact reservation (internal error)");
+    Pv->dev_gen++;
+}
+
+void render_deposit_collect(Render *r, const Particles *P) {
+    RenderPriv *Pv = rpriv(r);
+    const size_t need = Pv->total_host[0];
+    const unsigned over = Pv->total_host[1];
+    if (Pv->queued_est) {
+        if (over || need > Pv->rec_cap) deposit_exact(r, P, Pv);
+    } else {
+        if (over) fail_msg("render_deposit: a tile's sample records exceeded their exact reservation (internal error)");
+        if (need > Pv->rec_cap) {
+            dev_free(Pv->recs);
+            Pv->rec_cap = need + need / 4 + 1024;
+            Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
+            GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, stream()));
+            deposit_fill_tiles(r, P, Pv, Pv->queued);
+            GGB_CHECK(cudaStreamSynchronize(stream()));
+            Pv->dev_gen++;
+        }
+    }
+    Pv->have_prev = true;
 }
 
 void render_deposit_launch(Render *r, const Particles *P) {
@@ -1060,7 +1115,7 @@ GGB_EXPORT int render_init(Render *r, int R, float radius, float alpha) {
     Pv->tile_count = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_start = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_fill = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
-    Pv->diag = (unsigned *)dev_alloc(sizeof(unsigned) * 2);
+    Pv->diag = (unsigned *)dev_alloc(sizeof(unsigned) * 2);  // zeroed
     GGB_CHECK(cudaMallocHost(&Pv->total_host, sizeof(unsigned) * 2));
     Pv->total_host[0] = Pv->total_host[1] = 0;
     r->tr = reinterpret_cast<ThreadRecs *>(Pv);

@@ -630,3 +630,41 @@ def test_batched_step_fluid_only_planet(gpu):
     _batch_free(full)
     for w, x in zip(want, got):
         assert np.array_equal(w, x)
+
+
+def test_deposit_estimated_reservation_overflow_repeats(gpu, orc32):
+    """After a first deposit, each tile reserves slots from that deposit's
+    record counts.  A second deposit that packs 3000 particles into tiles the
+    first left empty (32 slots each) overflows them; the library repeats it
+    with exact reservations, so the faces equal the restatement's."""
+    R = 48
+    prev_a, pos_a, col_a = K.random_arcs(200, seed=31, max_angle=0.02)
+    rng = np.random.default_rng(32)
+    c = np.array([0.6, -0.6, 0.52])
+    c /= np.linalg.norm(c)
+    prev_b = c + 0.01 * rng.normal(size=(3000, 3))
+    prev_b /= np.linalg.norm(prev_b, axis=1, keepdims=True)
+    pos_b = prev_b + 0.004 * rng.normal(size=(3000, 3))
+    pos_b /= np.linalg.norm(pos_b, axis=1, keepdims=True)
+    col_b = rng.uniform(0.1, 1, size=(3000, 4))
+    out = {}
+    for name, api in (("gpu", gpu), ("orc", orc32)):
+        sets = []
+        for prev, pos, col in ((prev_a, pos_a, col_a), (prev_b, pos_b, col_b)):
+            ps = G.ParticleSet(api, len(prev))
+            ps.array("prev", 3)[:] = prev.astype(api.np_real)
+            ps.array("pos", 3)[:] = pos.astype(api.np_real)
+            ps.array("col", 4)[:] = col.astype(api.np_real)
+            sets.append(ps)
+        sp = G.Splat(api, R)
+        sp.fade(0.02)
+        sp.deposit(sets[0])
+        sp.fade(0.02)
+        sp.deposit(sets[1])
+        sp.fade(0.02)
+        sp.deposit(sets[0])  # reservations from the dense deposit, now oversized
+        out[name] = sp.faces()
+        sp.free()
+        for ps in sets:
+            ps.free()
+    assert np.max(np.abs(out["gpu"] - out["orc"])) <= 1e-6
