@@ -299,3 +299,37 @@ class Splat:
     def free(self):
         if self.r.buf:
             self.api.lib.render_free(C.byref(self.r))
+
+
+IMAGE_IO_LIB = os.path.join(HERE, "libggb_image_io.so")
+
+
+class ImageIO:
+    """PNG files through libggb_image_io.so (the upstream src/image_io.h API:
+    ``png_load_rgba``, ``png_save``)."""
+
+    def __init__(self, path=IMAGE_IO_LIB):
+        self.lib = C.CDLL(path)
+        self.lib.png_load_rgba.restype = C.POINTER(C.c_float)
+        self.lib.png_load_rgba.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        self.lib.png_save.restype = C.c_int
+        self.lib.png_save.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        self._free = C.CDLL(None).free
+        self._free.argtypes = [C.c_void_p]
+
+    def load(self, path):
+        """float32 array (h, w, 4) in [0, 1], or None when the file is rejected."""
+        w, h = C.c_int(0), C.c_int(0)
+        p = self.lib.png_load_rgba(os.fsencode(path), C.byref(w), C.byref(h))
+        if not p:
+            return None
+        try:
+            return np.ctypeslib.as_array(p, shape=(h.value * w.value * 4,)).copy().reshape(h.value, w.value, 4)
+        finally:
+            self._free(p)
+
+    def save(self, path, img):
+        """img: uint8 array (h, w, 3 or 4).  Returns png_save's status (0 or -1)."""
+        img = np.ascontiguousarray(img, dtype=np.uint8)
+        h, w, ch = img.shape
+        return self.lib.png_save(os.fsencode(path), w, h, ch, img.ctypes.data)

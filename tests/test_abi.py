@@ -1,5 +1,6 @@
-"""The C-ABI boundary, checked without a GPU: libggb_cuda.so loads, exports
-every function and data symbol that include/*.h declares, and the struct
+"""The C-ABI boundary, checked without a GPU: libggb_cuda.so loads and exports
+every function and data symbol that include/*.h declares (image_io.h's PNG
+functions: libggb_image_io.so), and the struct
 layouts of include/*.h equal those of the upstream headers (so callers built
 against either header share one ABI)."""
 import ctypes
@@ -33,11 +34,16 @@ def _strip_bodies(text):
     return "".join(out)
 
 
-def declared_symbols():
-    """Function names declared (not defined inline) in include/*.h, plus extern data."""
+# header -> the library that exports its functions (all others: libggb_cuda.so)
+OTHER_LIBS = {"image_io.h": ggb_api.IMAGE_IO_LIB}
+
+
+def declared_symbols(headers=None):
+    """Function names declared (not defined inline) in include/*.h (or in the
+    given header names), plus extern data."""
     funcs, data = set(), set()
     for fn in sorted(os.listdir(INCLUDE)):
-        if not fn.endswith(".h"):
+        if not fn.endswith(".h") or (headers is not None and fn not in headers):
             continue
         text = open(os.path.join(INCLUDE, fn)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
@@ -67,9 +73,14 @@ def test_headers_declare_the_upstream_api():
 def test_product_library_exports_every_declared_symbol():
     assert os.path.exists(ggb_api.PRODUCT_LIB), "build the library first (__graft_entry__.build())"
     lib = ctypes.CDLL(ggb_api.PRODUCT_LIB)
-    funcs, data = declared_symbols()
+    mine = [h for h in os.listdir(INCLUDE) if h.endswith(".h") and h not in OTHER_LIBS]
+    funcs, data = declared_symbols(mine)
     missing = [s for s in sorted(funcs | data) if not hasattr(lib, s)]
     assert not missing, missing
+    for header, path in OTHER_LIBS.items():
+        other = ctypes.CDLL(path)
+        funcs, _ = declared_symbols([header])
+        assert funcs and not [s for s in funcs if not hasattr(other, s)], (header, funcs)
 
 
 def test_product_library_has_no_cpu_fallback_symbols():
