@@ -92,17 +92,25 @@ __global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, co
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         D3 p = load3(pos + 3 * i), g = d3(0, 0, 0);
         double pi = psi[i];
-        int m = nnb[i];
-        for (int k = 0; k < m; k++) {
-            int j = __ldg(nbr + kMaxNb * i + k);
-            g = add(g, scale(load3(gc + 3 * (kMaxNb * i + k)), psi[j] - pi));
+        const int m = nnb[i];
+        // unrolled over the fixed neighbour capacity so that the neighbour
+        // gathers are in flight together; the sum keeps the order k = 0..m-1
+#pragma unroll
+        for (int k = 0; k < kMaxNb; k++) {
+            if (k < m) {
+                int j = __ldg(nbr + kMaxNb * i + k);
+                g = add(g, scale(load3(gc + 3 * (kMaxNb * i + k)), psi[j] - pi));
+            }
         }
         store3(vel + 3 * i, cross(p, g));
     }
 }
 
-// max |u|^2 (formed in FP32 like upstream src/fluid.c:480-491) as float bits.
-__global__ void k_max_speed2(int n, const float *vel, unsigned int *out) {
+// max |u|^2 (formed in FP32 like upstream src/fluid.c:480-491) into *out as the
+// bits of a non-negative float, so that the unsigned atomicMax orders them; one
+// atomic per block.
+__global__ void __launch_bounds__(kB) k_max_speed2(int n, const float *vel, unsigned int *out) {
+    __shared__ float s_m[kB / 32];
     float m = 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float *v = vel + 3 * i;
@@ -110,7 +118,13 @@ __global__ void k_max_speed2(int n, const float *vel, unsigned int *out) {
         m = fmaxf(m, s);
     }
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < kB / 32 ? s_m[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) atomicMax(out, __float_as_uint(m));
+    }
 }
 
 // The application driver's CFL step on the device (upstream src/main.c:422-426):
@@ -684,7 +698,7 @@ void fluid_cfl_dt_launch(const Fluid *F, double cfl, double *dt_dev) {
     cudaStream_t s = stream();
     const int n = F->cs->ncells;
     GGB_CHECK(cudaMemsetAsync(Pv->vmax_bits, 0, sizeof(unsigned int), s));
-    k_max_speed2<<<blocks_for(n), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
+    k_max_speed2<<<std::min(blocks_for(n), 2u * device_sm_count()), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
     GGB_LAUNCHED();
     k_cfl_dt<<<1, 1, 0, s>>>(Pv->vmax_bits, cfl, F->cs->h, dt_dev);
     GGB_LAUNCHED();
@@ -704,7 +718,7 @@ GGB_EXPORT double fluid_max_speed(const Fluid *F) {
     int n = F->cs->ncells;
     stage_begin(ST_MAXSPEED);
     GGB_CHECK(cudaMemsetAsync(Pv->vmax_bits, 0, sizeof(unsigned int), s));
-    k_max_speed2<<<blocks_for(n), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
+    k_max_speed2<<<std::min(blocks_for(n), 2u * device_sm_count()), kB, 0, s>>>(n, F->vel, Pv->vmax_bits);
     GGB_LAUNCHED();
     stage_end(ST_MAXSPEED);
     GGB_CHECK(cudaMemcpyAsync(Pv->vmax_host, Pv->vmax_bits, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
