@@ -71,9 +71,26 @@ __device__ __forceinline__ double get_total(const SolveParams &P, int which, dou
 
 // ---- staged stencil phases ------------------------------------------------
 
-__device__ __forceinline__ void block_range(int n, int &c0, int &c1) {
-    c0 = (int)(((long long)n * blockIdx.x) / gridDim.x);
-    c1 = (int)(((long long)n * (blockIdx.x + 1)) / gridDim.x);
+// This block's contiguous range of a level's n = 6 N^2 cells (face-major).
+// With at least 6 blocks every face gets a whole number of blocks (face f:
+// blocks [f nb / 6, (f + 1) nb / 6)) and splits its cells evenly among them,
+// so that no range holds the boundary rows of two faces: a range straddling a
+// face edge has twice the boundary-ring cells, which takes a second link pass
+// (or, at N = 512, another sub-range) and makes that block the phase's last.
+// Fewer blocks split the cells evenly.
+__device__ __forceinline__ void block_range(int n, int N, int &c0, int &c1) {
+    const int nb = gridDim.x, b = blockIdx.x;
+    if (nb < 6) {
+        c0 = (int)(((long long)n * b) / nb);
+        c1 = (int)(((long long)n * (b + 1)) / nb);
+        return;
+    }
+    int f = 0;
+    while (f < 5 && b >= ((f + 1) * nb) / 6) f++;
+    const int b0 = (f * nb) / 6, m = ((f + 1) * nb) / 6 - b0;
+    const long long nf = (long long)N * N;
+    c0 = (int)(f * nf + nf * (b - b0) / m);
+    c1 = (int)(f * nf + nf * (b - b0 + 1) / m);
 }
 
 __device__ unsigned long long *g_stage_trace;  // diagnostics: block 0 stamps staging / compute ends
@@ -119,7 +136,7 @@ template <class Load, class Commit, class Cell>
 __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load load, Commit commit, Cell cell) {
     const int N = S.N, n = S.n, nring = S.nring, bs = blockDim.x, tid = threadIdx.x;
     int c0, c1;
-    block_range(n, c0, c1);
+    block_range(n, N, c0, c1);
     const int halo = N + 1;
     const int sub = kStageCap - 2 * halo;
     double *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap,
