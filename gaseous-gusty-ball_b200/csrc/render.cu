@@ -379,57 +379,74 @@ __global__ void __launch_bounds__(256, 5)
     }
 }
 
-// Exclusive scan of cnt[0..n) into start[0..n] (one block of 1024 threads).
-// The counts of up to 32 chunks of 1024 are loaded at once (coalesced, one
-// memory latency), then scanned chunk after chunk with warp shuffles.
+// Exclusive scan of cnt[0..n) into start[0..n] and *total (one block of 1024
+// threads).  Each thread owns a contiguous segment of the counts, a multiple of
+// four long (16-byte loads and stores; cnt and start are 16-byte aligned): it
+// sums its segment, the block scans the 1024 sums (one barrier per level of a
+// two-level warp scan), and the thread writes its segment's prefixes.
 // est: the counts are the previous deposit's record counts, and each tile
 // reserves that count plus half of it plus 32 (records of a tile change little
 // from one step to the next; a tile that still overflows makes the deposit
 // repeat with exact reservations).
+__device__ __forceinline__ unsigned tile_reserve(unsigned x, int est) { return est ? x + x / 2 + 32u : x; }
+
 __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, int est, unsigned *start,
                                                    unsigned *total) {
-    constexpr int kChunks = 32;
     __shared__ unsigned s_w[32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    unsigned carry = 0;
-    for (int g0 = 0; g0 < n; g0 += kChunks * 1024) {
-        unsigned v[kChunks];
+    const int per = (((n + 1023) / 1024) + 3) & ~3;
+    const int a = min(n, t * per), b = min(n, a + per);
+    const uint4 *c4 = reinterpret_cast<const uint4 *>(cnt);
+    unsigned sum = 0;
+    int i = a;
+#pragma unroll 4
+    for (; i + 4 <= b; i += 4) {
+        const uint4 v = c4[i >> 2];
+        sum += tile_reserve(v.x, est) + tile_reserve(v.y, est) + tile_reserve(v.z, est) + tile_reserve(v.w, est);
+    }
+    for (int k = i; k < b; k++) sum += tile_reserve(cnt[k], est);
+    unsigned x = sum;
 #pragma unroll
-        for (int c = 0; c < kChunks; c++) {
-            const int i = g0 + c * 1024 + t;
-            const unsigned x = i < n ? cnt[i] : 0u;
-            v[c] = i < n ? (est ? x + x / 2 + 32u : x) : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned w = s_w[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-#pragma unroll
-        for (int c = 0; c < kChunks; c++) {
-            if (g0 + c * 1024 >= n) break;
-            unsigned x = v[c];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (lane == 31) s_w[warp] = x;
-            __syncthreads();
-            if (warp == 0) {
-                unsigned w = s_w[lane];
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
-                    if (lane >= o) w += y;
-                }
-                s_w[lane] = w;
-            }
-            __syncthreads();
-            const int i = g0 + c * 1024 + t;
-            if (i < n) start[i] = carry + (warp ? s_w[warp - 1] : 0u) + x - v[c];
-            carry += s_w[31];
-            __syncthreads();
-        }
+        s_w[lane] = w;
+    }
+    __syncthreads();
+    unsigned run = (warp ? s_w[warp - 1] : 0u) + x - sum;
+    uint4 *s4 = reinterpret_cast<uint4 *>(start);
+    i = a;
+#pragma unroll 4
+    for (; i + 4 <= b; i += 4) {
+        const uint4 v = c4[i >> 2];
+        uint4 o;
+        o.x = run;
+        run += tile_reserve(v.x, est);
+        o.y = run;
+        run += tile_reserve(v.y, est);
+        o.z = run;
+        run += tile_reserve(v.z, est);
+        o.w = run;
+        run += tile_reserve(v.w, est);
+        s4[i >> 2] = o;
+    }
+    for (int k = i; k < b; k++) {
+        start[k] = run;
+        run += tile_reserve(cnt[k], est);
     }
     if (t == 0) {
-        start[n] = carry;
-        *total = carry;
+        start[n] = s_w[31];
+        *total = s_w[31];
     }
 }
 
