@@ -93,14 +93,27 @@ __global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, co
         D3 p = load3(pos + 3 * i), g = d3(0, 0, 0);
         double pi = psi[i];
         const int m = nnb[i];
-        // unrolled over the fixed neighbour capacity so that the neighbour
-        // gathers are in flight together; the sum keeps the order k = 0..m-1
+        // the cell's 8 neighbour slots and 24 coefficients (rows padded to
+        // kMaxNb, 16-byte aligned) as 16-byte loads; unrolled over the slots
+        // so that the psi gathers are in flight together; the sum keeps the
+        // order k = 0..m-1
+        static_assert(kMaxNb == 8, "a row is two int4 slots and six float4 coefficients");
+        const int4 *n4 = reinterpret_cast<const int4 *>(nbr + (size_t)kMaxNb * i);
+        const float4 *g4 = reinterpret_cast<const float4 *>(gc + (size_t)3 * kMaxNb * i);
+        const int4 na = __ldg(n4), nb = __ldg(n4 + 1);
+        const int jj[kMaxNb] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+        float gv[3 * kMaxNb];
+#pragma unroll
+        for (int u = 0; u < 6; u++) {
+            const float4 q = __ldg(g4 + u);
+            gv[4 * u] = q.x;
+            gv[4 * u + 1] = q.y;
+            gv[4 * u + 2] = q.z;
+            gv[4 * u + 3] = q.w;
+        }
 #pragma unroll
         for (int k = 0; k < kMaxNb; k++) {
-            if (k < m) {
-                int j = __ldg(nbr + kMaxNb * i + k);
-                g = add(g, scale(load3(gc + 3 * (kMaxNb * i + k)), psi[j] - pi));
-            }
+            if (k < m) g = add(g, scale(d3(gv[3 * k], gv[3 * k + 1], gv[3 * k + 2]), psi[jj[k]] - pi));
         }
         store3(vel + 3 * i, cross(p, g));
     }
