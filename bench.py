@@ -361,6 +361,7 @@ def run_ours(a, rank, world, local):
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world} (one planet per GPU)",
                        "l2": working_set_note(CFG),
                        "mean_cg_iters": kit,
+                       "deposit_repeats": int(api.lib.ggb_render_repeats(C.byref(pl.sp.r))),
                        "stage_ms_per_step": {k: v[0] / KS for k, v in per_stage.items()},
                        "stage_steps": KS},
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -527,6 +528,7 @@ def run_batch(a, rank, world, local):
                        "psi_error": "batched and plain run the same FP32 solve to the same tolerance",
                        "cells_per_block": best, "tuning_ms_per_step": {str(k): v for k, v in tried.items()},
                        "host_ms_last_step": host_ms,
+                       "deposit_repeats": int(sum(api.lib.ggb_render_repeats(C.byref(p[3].r)) for p in planets)),
                        "timing": "max of CUDA events on the library stream and the host wall clock"},
             "clocks": clocks}), flush=True)
     for g, fs, ps, spl, sp in planets:

@@ -62,6 +62,9 @@ struct RenderPriv {
     SplatCfg queued{};             // configuration of the last queued deposit (for its repeat)
     bool queued_est = false;       // its slots were estimated from the previous deposit's fills
     bool have_prev = false;        // tile_fill holds the previous deposit's record counts
+    unsigned long repeats = 0;     // times a deposit's fill and compositing ran again
+    int exact_next = 0;            // deposits still to reserve exactly after an estimate overflowed
+    int backoff = 1;               // exact deposits after the next overflow (doubles up to 64)
     float *mirror = nullptr;
     unsigned char *enc = nullptr;  // device scratch of the 8-bit encoders (host outputs)
     size_t enc_cap = 0;
@@ -831,16 +834,24 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
 // scan, fill and compositing and the copies of the reserved total and the
 // overflow count.  The reservation is exact (k_rd_count) for the first deposit
 // and estimated from the previous deposit's per-tile record counts afterwards
-// (no counting pass).  render_deposit_collect (after a synchronisation of the
-// stream) checks the outcome: when the record buffer was too small or an
-// estimated tile overflowed, fill and compositing skipped (the face buffer is
-// untouched) and the deposit is repeated with exact reservations.
+// (no counting pass), except for the b deposits after an estimate overflowed
+// (b doubles with every overflow up to 64 and halves with every estimate that
+// fits).  render_deposit_collect (after a synchronisation of the
+// stream) checks the outcome.  Fill and compositing skip the whole deposit
+// (the face buffer is untouched) when the record buffer was too small, and
+// compositing skips it when an estimated tile overflowed.  The host then grows
+// the buffer and runs them again on the same reservations, or repeats the
+// deposit with exact reservations.
 void render_deposit_queue(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
-    const bool est = Pv->have_prev;
+    // estimated reservations unless a recent estimate overflowed (a sparse
+    // planet's tile counts can jump from one step to the next; each overflow
+    // costs a repeated deposit, each exact reservation only the counting pass)
+    const bool est = Pv->have_prev && Pv->exact_next == 0;
+    if (Pv->have_prev && !est) Pv->exact_next--;
     stage_begin(ST_BIN);
     GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
     if (est) {
@@ -868,9 +879,36 @@ void render_deposit_queue(Render *r, const Particles *P) {
     Pv->dev_gen++;
 }
 
+// Grows the record buffer to hold need records, with room for the next
+// deposit's estimated reservation (at most 1.5 x this deposit's records plus
+// 32 per tile).  Without that room a sparse planet, whose estimate is mostly
+// the 32 slots per tile, would outgrow the buffer at every deposit.
+static void grow_records(RenderPriv *Pv, size_t need) {
+    if (need <= Pv->rec_cap) return;
+    dev_free(Pv->recs);
+    Pv->rec_cap = need + need / 2 + (size_t)32 * Pv->ntiles + 1024;
+    Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
+}
+
+// Fill and compositing of the queued deposit again, with the reservations
+// already in tile_start (synchronous; after the record buffer grew).  Returns
+// the tile overflow flag.
+static unsigned deposit_refill(Render *r, const Particles *P, RenderPriv *Pv) {
+    cudaStream_t s = stream();
+    Pv->repeats++;
+    GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
+    GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
+    deposit_fill_tiles(r, P, Pv, Pv->queued);
+    GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    GGB_CHECK(cudaStreamSynchronize(s));
+    Pv->dev_gen++;
+    return Pv->total_host[1];
+}
+
 // The queued deposit again with exact reservations (synchronous).
 static void deposit_exact(Render *r, const Particles *P, RenderPriv *Pv) {
     cudaStream_t s = stream();
+    Pv->repeats++;
     const SplatCfg &C = Pv->queued;
     const int n = P->n;
     GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
@@ -884,12 +922,7 @@ static void deposit_exact(Render *r, const Particles *P, RenderPriv *Pv) {
     GGB_LAUNCHED();
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaStreamSynchronize(s));
-    const size_t need = Pv->total_host[0];
-    if (need > Pv->rec_cap) {
-        dev_free(Pv->recs);
-        Pv->rec_cap = need + need / 4 + 1024;
-        Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
-    }
+    grow_records(Pv, Pv->total_host[0]);
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
     deposit_fill_tiles(r, P, Pv, C);
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host + 1, Pv->diag + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -902,20 +935,21 @@ static void deposit_exact(Render *r, const Particles *P, RenderPriv *Pv) {
 void render_deposit_collect(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     const size_t need = Pv->total_host[0];
-    const unsigned over = Pv->total_host[1];
+    unsigned over = Pv->total_host[1];
+    if (need > Pv->rec_cap) {  // fill and compositing were skipped: grow the buffer, run them again
+        grow_records(Pv, need);
+        over = deposit_refill(r, P, Pv);
+    }
     if (Pv->queued_est) {
-        if (over || need > Pv->rec_cap) deposit_exact(r, P, Pv);
-    } else {
-        if (over) fail_msg("render_deposit: a tile's sample records exceeded their exact reservation (internal error)");
-        if (need > Pv->rec_cap) {
-            dev_free(Pv->recs);
-            Pv->rec_cap = need + need / 4 + 1024;
-            Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
-            GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, stream()));
-            deposit_fill_tiles(r, P, Pv, Pv->queued);
-            GGB_CHECK(cudaStreamSynchronize(stream()));
-            Pv->dev_gen++;
+        if (over) {  // a tile outgrew its estimate: exact reservations, for this and the next deposits
+            Pv->exact_next = Pv->backoff;
+            Pv->backoff = std::min(2 * Pv->backoff, 64);
+            deposit_exact(r, P, Pv);
+        } else {
+            Pv->backoff = std::max(1, Pv->backoff / 2);
         }
+    } else if (over) {
+        fail_msg("render_deposit: a tile's sample records exceeded their exact reservation (internal error)");
     }
     Pv->have_prev = true;
 }
@@ -1259,6 +1293,11 @@ GGB_EXPORT void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *sl
     if (slow_tiles) *slow_tiles = sc;
     if (entries) *entries = Pv->total_host[0];
 }
+
+// Additive diagnostics: how many times the fill and compositing of this
+// Render's deposits ran again (record buffer grown, or an estimated tile
+// reservation overflowed).
+GGB_EXPORT unsigned long ggb_render_repeats(const Render *r) { return rpriv(r)->repeats; }
 
 // Additive: the application driver's 8-bit images, encoded on the GPU (upstream
 // src/main.c:249-318).  bg == NULL: transparent (RGBA, un-premultiplied);

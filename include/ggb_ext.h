@@ -55,6 +55,10 @@ void ggb_render_read(const Render *r, float *out);
  * composited in several key-range windows, and the record slots reserved for
  * (sample, tile) records. */
 void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, unsigned *entries);
+/* Diagnostics: how many times the fill and compositing of this Render's
+ * deposits ran again (the record buffer grew, or a tile outgrew its estimated
+ * reservation). */
+unsigned long ggb_render_repeats(const Render *r);
 
 /* The application driver's 8-bit output images (its write_outputs), encoded
  * on the GPU from the face buffer: render_texel then render_pixel8 per texel.

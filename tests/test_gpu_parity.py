@@ -668,3 +668,50 @@ def test_deposit_estimated_reservation_overflow_repeats(gpu, orc32):
         for ps in sets:
             ps.free()
     assert np.max(np.abs(out["gpu"] - out["orc"])) <= 1e-6
+
+
+def test_deposit_overflow_backoff(gpu, orc32):
+    """After an estimated reservation overflows, the next deposits reserve
+    exactly (one, then two, then four ...: the count doubles with every
+    overflow and halves with every estimate that fits), so a planet whose tile
+    counts keep jumping does not repeat every deposit.  Alternating a sparse
+    and a dense particle set: the dense deposit overflows whenever it is
+    estimated from the sparse one.  The faces still equal the restatement's."""
+    R = 48
+    prev_a, pos_a, col_a = K.random_arcs(200, seed=31, max_angle=0.02)
+    rng = np.random.default_rng(32)
+    c = np.array([0.6, -0.6, 0.52])
+    c /= np.linalg.norm(c)
+    prev_b = c + 0.01 * rng.normal(size=(3000, 3))
+    prev_b /= np.linalg.norm(prev_b, axis=1, keepdims=True)
+    pos_b = prev_b + 0.004 * rng.normal(size=(3000, 3))
+    pos_b /= np.linalg.norm(pos_b, axis=1, keepdims=True)
+    col_b = rng.uniform(0.1, 1, size=(3000, 4))
+    # deposit:           a  b  a  b  a  b  a  b
+    # reservation:       x  e  x  e  x  x  e  e   (x exact, e estimated)
+    # repeats: the first deposit grows the record buffer, every estimated b
+    # overflows (cumulative count after each deposit)
+    expect_repeats = [1, 2, 2, 3, 3, 3, 3, 4]
+    out = {}
+    for name, api in (("gpu", gpu), ("orc", orc32)):
+        sets = []
+        for prev, pos, col in ((prev_a, pos_a, col_a), (prev_b, pos_b, col_b)):
+            ps = G.ParticleSet(api, len(prev))
+            ps.array("prev", 3)[:] = prev.astype(api.np_real)
+            ps.array("pos", 3)[:] = pos.astype(api.np_real)
+            ps.array("col", 4)[:] = col.astype(api.np_real)
+            sets.append(ps)
+        sp = G.Splat(api, R)
+        got = []
+        for k in range(len(expect_repeats)):
+            sp.fade(0.02)
+            sp.deposit(sets[k % 2])
+            if name == "gpu":
+                got.append(int(api.lib.ggb_render_repeats(C.byref(sp.r))))
+        if name == "gpu":
+            assert got == expect_repeats, got
+        out[name] = sp.faces()
+        sp.free()
+        for ps in sets:
+            ps.free()
+    assert np.max(np.abs(out["gpu"] - out["orc"])) <= 1e-6
