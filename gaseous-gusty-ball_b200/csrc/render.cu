@@ -383,73 +383,92 @@ __global__ void __launch_bounds__(256, 5)
 }
 
 // Exclusive scan of cnt[0..n) into start[0..n] and *total (one block of 1024
-// threads).  Each thread owns a contiguous segment of the counts, a multiple of
-// four long (16-byte loads and stores; cnt and start are 16-byte aligned): it
-// sums its segment, the block scans the 1024 sums (one barrier per level of a
-// two-level warp scan), and the thread writes its segment's prefixes.
+// threads).  Each warp owns a contiguous segment of the counts (a multiple of
+// 128 long; cnt and start are 16-byte aligned) and walks it 128 counts at a
+// time, a 16-byte load per lane (coalesced): a first pass sums the segment,
+// the block scans the 32 warp sums, a second pass writes the prefixes (a warp
+// scan per step, the running total carried from step to step).
 // est: the counts are the previous deposit's record counts, and each tile
 // reserves that count plus half of it plus 32 (records of a tile change little
 // from one step to the next; a tile that still overflows makes the deposit
 // repeat with exact reservations).
 __device__ __forceinline__ unsigned tile_reserve(unsigned x, int est) { return est ? x + x / 2 + 32u : x; }
 
+// Counts i..i+3 (zero past n), transformed by tile_reserve.
+__device__ __forceinline__ uint4 tile_load4(const unsigned *cnt, int i, int n, int est) {
+    uint4 v;
+    if (i + 4 <= n) {
+        v = reinterpret_cast<const uint4 *>(cnt)[i >> 2];
+    } else {
+        v.x = i < n ? cnt[i] : 0u;
+        v.y = i + 1 < n ? cnt[i + 1] : 0u;
+        v.z = i + 2 < n ? cnt[i + 2] : 0u;
+        v.w = i + 3 < n ? cnt[i + 3] : 0u;
+    }
+    if (i < n) {
+        v.x = tile_reserve(v.x, est);
+        v.y = i + 1 < n ? tile_reserve(v.y, est) : 0u;
+        v.z = i + 2 < n ? tile_reserve(v.z, est) : 0u;
+        v.w = i + 3 < n ? tile_reserve(v.w, est) : 0u;
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, int est, unsigned *start,
                                                    unsigned *total) {
     __shared__ unsigned s_w[32];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int per = (((n + 1023) / 1024) + 3) & ~3;
-    const int a = min(n, t * per), b = min(n, a + per);
-    const uint4 *c4 = reinterpret_cast<const uint4 *>(cnt);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = ((n + 31) / 32 + 127) & ~127;
+    const int w0 = min(n, warp * seg), w1 = min(n, w0 + seg);
     unsigned sum = 0;
-    int i = a;
 #pragma unroll 4
-    for (; i + 4 <= b; i += 4) {
-        const uint4 v = c4[i >> 2];
-        sum += tile_reserve(v.x, est) + tile_reserve(v.y, est) + tile_reserve(v.z, est) + tile_reserve(v.w, est);
+    for (int b = w0; b < w1; b += 128) {
+        const uint4 v = tile_load4(cnt, b + 4 * lane, w1, est);
+        sum += v.x + v.y + v.z + v.w;
     }
-    for (int k = i; k < b; k++) sum += tile_reserve(cnt[k], est);
-    unsigned x = sum;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_w[warp] = x;
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) s_w[warp] = sum;
     __syncthreads();
     if (warp == 0) {
-        unsigned w = s_w[lane];
+        const unsigned x = s_w[lane];
+        unsigned incl = x;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        s_w[lane] = w;
+        s_w[lane] = incl - x;  // exclusive: the counts before this warp's segment
+        if (lane == 31) {
+            start[n] = incl;
+            *total = incl;
+        }
     }
     __syncthreads();
-    unsigned run = (warp ? s_w[warp - 1] : 0u) + x - sum;
-    uint4 *s4 = reinterpret_cast<uint4 *>(start);
-    i = a;
-#pragma unroll 4
-    for (; i + 4 <= b; i += 4) {
-        const uint4 v = c4[i >> 2];
-        uint4 o;
-        o.x = run;
-        run += tile_reserve(v.x, est);
-        o.y = run;
-        run += tile_reserve(v.y, est);
-        o.z = run;
-        run += tile_reserve(v.z, est);
-        o.w = run;
-        run += tile_reserve(v.w, est);
-        s4[i >> 2] = o;
-    }
-    for (int k = i; k < b; k++) {
-        start[k] = run;
-        run += tile_reserve(cnt[k], est);
-    }
-    if (t == 0) {
-        start[n] = s_w[31];
-        *total = s_w[31];
+    unsigned carry = s_w[warp];
+    for (int b = w0; b < w1; b += 128) {
+        const int i = b + 4 * lane;
+        const uint4 v = tile_load4(cnt, i, w1, est);
+        const unsigned t = v.x + v.y + v.z + v.w;
+        unsigned incl = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint4 o4;
+        o4.x = carry + incl - t;
+        o4.y = o4.x + v.x;
+        o4.z = o4.y + v.y;
+        o4.w = o4.z + v.z;
+        if (i + 4 <= w1) {
+            reinterpret_cast<uint4 *>(start)[i >> 2] = o4;
+        } else {
+            if (i < w1) start[i] = o4.x;
+            if (i + 1 < w1) start[i + 1] = o4.y;
+            if (i + 2 < w1) start[i + 2] = o4.z;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
 }
 
