@@ -519,10 +519,23 @@ __device__ __forceinline__ unsigned short rec_box(const SplatCfg &C, const TileG
 __device__ __forceinline__ int box_entries(unsigned short b) {
     return b == kNoBox ? 0 : ((b >> 8 & 15) + 1) * ((b >> 12) + 1);
 }
+// f(texel) for each texel of box b.  Boxes of at most 2 x 2 texels (every box
+// when the splat radius is 1 or less: a positive weight needs |x - px| < r)
+// take a straight-line path; the visiting order does not matter to callers.
 template <class F>
 __device__ __forceinline__ void box_texels(unsigned short b, F f) {
     if (b == kNoBox) return;
     const int x0 = b & 15, y0 = b >> 4 & 15, w = (b >> 8 & 15) + 1, h = (b >> 12) + 1;
+    if (w <= 2 && h <= 2) {
+        const int t = y0 * kT + x0;
+        f(t);
+        if (w == 2) f(t + 1);
+        if (h == 2) {
+            f(t + kT);
+            if (w == 2) f(t + kT + 1);
+        }
+        return;
+    }
     for (int y = y0; y < y0 + h; y++)
         for (int x = x0; x < x0 + w; x++) f(y * kT + x);
 }
