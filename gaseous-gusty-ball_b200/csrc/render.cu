@@ -477,6 +477,7 @@ constexpr int kTB = kT * kT;   // threads per tile block: one texel each
 constexpr int kRec = 768;      // records of one window (shared memory)
 constexpr int kEnt = 2304;     // (record, texel) entries of one window
 constexpr int kHist = 1024;    // key buckets when a dense tile is cut into windows
+constexpr int kBucket = 16;    // entry slots per texel of the one-pass path
 
 struct TileSmem {
     union {
@@ -488,12 +489,15 @@ struct TileSmem {
     } u;
     float4 col[kRec];
     unsigned short box[kRec];
-    unsigned short ent[kEnt];
+    union {
+        unsigned short ent[kEnt];                 // entry lists packed by a count scan
+        unsigned short bucket[kT * kT * kBucket];  // kBucket entry slots per texel (one-pass path)
+    };
     int cnt[kT * kT];
     int start[kT * kT];
     unsigned long long scan_w[kTB / 32];
     int wsum[kTB / 32];
-    int cut, tot;
+    int cut, tot, full;
 };
 
 struct TileGeo {
@@ -773,9 +777,14 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
     }
     if (m > 0) {
         const Rec *Rt = recs + s0;
-        // one window: records and per-texel counts in one pass
+        // one window: records, per-texel counts and, while no texel takes more
+        // than kBucket entries, the entries themselves (each in the slot its
+        // count gives it) in one pass
         S.cnt[q] = 0;
-        if (q == 0) S.tot = 0;
+        if (q == 0) {
+            S.tot = 0;
+            S.full = 0;
+        }
         __syncthreads();
         if (m <= kRec) {
             int e = 0;
@@ -783,7 +792,13 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
                 const Rec r = Rt[s];
                 const unsigned short box = rec_box(C, G, r.px, r.py);
                 window_put(S, s, r, box);
-                box_texels(box, [&](int t) { atomicAdd(&S.cnt[t], 1); });
+                box_texels(box, [&](int t) {
+                    const int k = atomicAdd(&S.cnt[t], 1);
+                    if (k < kBucket)
+                        S.bucket[t * kBucket + k] = (unsigned short)s;
+                    else
+                        S.full = 1;
+                });
                 e += box_entries(box);
             }
 #pragma unroll
@@ -791,7 +806,11 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
             if ((q & 31) == 0 && e) atomicAdd(&S.tot, e);
         }
         __syncthreads();
-        if (m <= kRec && S.tot <= kEnt) {
+        if (m <= kRec && !S.full) {
+            const int c = S.cnt[q];
+            if (c) blend_texel(S, S.bucket + q * kBucket, c, q, C, G, d);
+        } else if (m <= kRec && S.tot <= kEnt) {
+            // a texel with more than kBucket entries: pack the lists by a count scan
             const int c = S.cnt[q];
             const int st = block_scan_1sync(c, S.wsum);
             S.start[q] = st;

@@ -275,6 +275,25 @@ def test_deposit_long_arcs_few_particles(gpu, orc32):
     assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
 
 
+def test_deposit_crowded_texels_one_window(gpu, orc32):
+    """300 particles with one sample each inside a single texel: the tile's
+    records fit one window, but that texel's entries overflow the per-texel
+    slots of the one-pass path, so the lists are packed by a count scan."""
+    rng = np.random.default_rng(21)
+    n = 300
+    c = np.array([0.31, -0.22, 0.92])
+    c /= np.linalg.norm(c)
+    prev = c + 2e-4 * rng.normal(size=(n, 3))
+    prev /= np.linalg.norm(prev, axis=1, keepdims=True)
+    pos = prev + 1e-6 * rng.normal(size=(n, 3))
+    pos /= np.linalg.norm(pos, axis=1, keepdims=True)
+    col = rng.uniform(0.1, 1, size=(n, 4))
+    a = K.deposit(gpu, 96, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    b = K.deposit(orc32, 96, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32))
+    assert a["windowed"] == 0
+    assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
+
+
 def test_fade_renormalisation(gpu, orc32):
     """g falls below 1e-4 (the buffer is rescaled, fused into the next deposit)."""
     prev, pos, col = K.random_arcs(500, seed=5, max_angle=0.05)
