@@ -303,24 +303,29 @@ def run_ours(a, rank, world, local):
     host_faces = torch.empty(face_bytes, dtype=torch.uint8).pin_memory().numpy()
     host_ptr = host_faces.ctypes.data_as(C.POINTER(C.c_ubyte))
     every = CFG["every"]
-    if api.lib.ggb_checkpoint_load(ckpt, C.byref(pl.fs.F), C.byref(pl.ps.P), C.byref(pl.sp.r)) != 0:
-        raise RuntimeError("bench: restoring the planet failed")
+    # three runs of the loop, each from the checkpoint; the median is reported
+    # (a single host stall of the wall clock would otherwise move the figure)
+    e2e_runs = []
+    for _ in range(3):
+        if api.lib.ggb_checkpoint_load(ckpt, C.byref(pl.fs.F), C.byref(pl.ps.P), C.byref(pl.sp.r)) != 0:
+            raise RuntimeError("bench: restoring the planet failed")
+        barrier()
+        api.lib.ggb_timer_start()
+        t0 = time.perf_counter()
+        reads = 0
+        for s in range(1, K + 1):
+            pl.step()
+            if s % every == 0 or s == K:
+                api.lib.ggb_encode_faces(C.byref(pl.sp.r), None, None, host_ptr)
+                reads += 1
+        e2e_ms = api.lib.ggb_timer_stop()
+        e2e_wall = time.perf_counter() - t0
+        barrier()
+        e2e_ms = max_over_ranks(max(e2e_ms, 1000 * e2e_wall))
+        e2e_runs.append(world * K / (e2e_ms / 1000.0))
     os.remove(ckpt)
     os.rmdir(ckpt_dir)
-    barrier()
-    api.lib.ggb_timer_start()
-    t0 = time.perf_counter()
-    reads = 0
-    for s in range(1, K + 1):
-        pl.step()
-        if s % every == 0 or s == K:
-            api.lib.ggb_encode_faces(C.byref(pl.sp.r), None, None, host_ptr)
-            reads += 1
-    e2e_ms = api.lib.ggb_timer_stop()
-    e2e_wall = time.perf_counter() - t0
-    barrier()
-    e2e_ms = max_over_ranks(max(e2e_ms, 1000 * e2e_wall))
-    e2e = world * K / (e2e_ms / 1000.0)
+    e2e = statistics.median(e2e_runs)
 
     # ---- roofline of the dominant stage (CUDA events on the library stream)
     n = pl.g.n
@@ -366,8 +371,10 @@ def run_ours(a, rank, world, local):
                        "stage_steps": KS},
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(8 + 32 + reads * face_bytes / K),
-                    "note": "C-ABI loop of the application driver over the same K steps as value (state "
-                            "restored from a checkpoint taken before the value loop): per step the max-speed "
+                    "runs": e2e_runs,
+                    "note": "median of three runs of the C-ABI loop of the application driver over the same K "
+                            "steps as value (state restored from a checkpoint taken before the value loop, "
+                            "before each run): per step the max-speed "
                             "(8 B) and solve status (32 B) read-backs; every 100 steps and at the last step the "
                             "six faces encoded on the GPU as 8-bit RGBA (the driver's default output) and copied "
                             "to pinned host memory; no per-step host inputs (state stays on the GPU)"},
