@@ -291,7 +291,21 @@ __device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, fl
     r.col = col;
     for (int u = 0; u < most; u++) {
         const bool on = u < ntxs * ntys;
-        const int tl = on ? (f * C.ntx + ty0 + u / ntxs) * C.ntx + tx0 + u % ntxs : 0;
+        // tile u of the footprint's ntxs x ntys tiles, row-major (a footprint
+        // of radius <= 1 spans at most two tiles per axis: shifts, no division)
+        int dy = 0, dx = 0;
+        if (on) {
+            if (ntxs == 1) {
+                dy = u;
+            } else if (ntxs == 2) {
+                dy = u >> 1;
+                dx = u & 1;
+            } else {
+                dy = u / ntxs;
+                dx = u - dy * ntxs;
+            }
+        }
+        const int tl = on ? (f * C.ntx + ty0 + dy) * C.ntx + tx0 + dx : 0;
         append_rec(tl, on, r, tile_start, tile_fill, recs, diag);
     }
 }
