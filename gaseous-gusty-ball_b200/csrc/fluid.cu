@@ -323,6 +323,9 @@ static StencilDev stencil_of(const GridTables *t) {
     s.N = t->N;
     s.n = t->n;
     s.nring = t->nring;
+    s.lgN = -1;
+    for (int l = 0; l < 31; l++)
+        if ((1 << l) == t->N) s.lgN = l;
     s.wslot = t->wslot;
     s.wslot_d = t->wslot_d;
     s.ring_nb = t->ring_nb;

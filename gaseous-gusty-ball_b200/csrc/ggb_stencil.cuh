@@ -10,6 +10,7 @@ namespace ggb {
 
 struct StencilDev {
     int N, n, nring;
+    int lgN;              // log2(N) when N is a power of two, else -1
     const float *wslot;   // [4][n]: E, N, NE, NW weights (0 = no link)
     const double *wslot_d;  // the same in FP64
     const int *ring_nb;   // [6*nring][8], -1 terminated
@@ -29,6 +30,20 @@ __device__ __forceinline__ void cell_fij(int c, int N, int &f, int &i, int &j) {
     int rem = c - f * nn;
     j = rem / N;
     i = rem - j * N;
+}
+
+// cell_fij for a level's stencil: shifts and masks when N is a power of two
+// (an integer division takes some twenty instructions), the division otherwise.
+__device__ __forceinline__ void cell_fij(const StencilDev &S, int c, int &f, int &i, int &j) {
+    const int l = S.lgN;
+    if (l >= 0) {
+        f = c >> (2 * l);
+        const int rem = c & ((1 << (2 * l)) - 1);
+        j = rem >> l;
+        i = rem & ((1 << l) - 1);
+    } else {
+        cell_fij(c, S.N, f, i, j);
+    }
 }
 
 // The links of a boundary-ring cell that leave the face: all eight (neighbour,
@@ -63,7 +78,7 @@ template <class X>
 __device__ __forceinline__ double apply_k(const StencilDev &S, int c, double xc, X X_) {
     const int N = S.N, n = S.n;
     int f, i, j;
-    cell_fij(c, N, f, i, j);
+    cell_fij(S, c, f, i, j);
     const float *ws = S.wslot;
     if (i > 0 && j > 0 && i + 1 < N && j + 1 < N) {
         const float w0 = __ldg(ws + c), w1 = __ldg(ws + n + c), w2 = __ldg(ws + 2 * n + c),
@@ -131,7 +146,7 @@ __device__ __forceinline__ double apply_k_smem(const StencilDev &S, int c, doubl
                                                const double *wNW, const double *rsum, int r0) {
     const int N = S.N;
     int f, i, j;
-    cell_fij(c, N, f, i, j);
+    cell_fij(S, c, f, i, j);
     double s = wE[c] * (xc - x[c + 1]);
     s += wN[c] * (xc - x[c + N]);
     s += wNE[c] * (xc - x[c + N + 1]);
@@ -149,7 +164,7 @@ __device__ __forceinline__ double apply_k_smem(const StencilDev &S, int c, doubl
 __device__ __forceinline__ void cell_links(const StencilDev &S, int c, int nb[kMaxNb], float wv[kMaxNb]) {
     const int N = S.N, n = S.n;
     int f, i, j;
-    cell_fij(c, N, f, i, j);
+    cell_fij(S, c, f, i, j);
     const float *ws = S.wslot;
     int m = 0;
     auto put = [&](int o, float q) {

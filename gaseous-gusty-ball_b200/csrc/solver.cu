@@ -299,7 +299,7 @@ __device__ __forceinline__ float presmooth_x(const LevelDev &L, int k, float b) 
 __device__ __forceinline__ float restrict_value(const LevelDev &F, const LevelDev &C, int c) {
     const int Nc = C.S.N, Nf = F.S.N;
     int f, I, J;
-    cell_fij(c, Nc, f, I, J);
+    cell_fij(C.S, c, f, I, J);
     double acc = 0;
     if (F.structured && I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc) {
         const float *r = F.r;
@@ -334,7 +334,7 @@ __device__ __forceinline__ float prolong_value(const LevelDev &F, const LevelDev
     const float *xc = C.xo;
     int t0, t1, t2, t3;
     int f, fi, fj;
-    cell_fij(i, Nf, f, fi, fj);
+    cell_fij(F.S, i, f, fi, fj);
     const int I0 = (fi - 1) >> 1, J0 = (fj - 1) >> 1;
     if (F.structured && I0 >= 0 && J0 >= 0 && I0 + 1 < Nc && J0 + 1 < Nc) {
         t0 = (f * Nc + J0) * Nc + I0;
@@ -891,7 +891,7 @@ __global__ void k_build_rw16(LevelDev F, LevelDev C, float *rw16) {
     const int Nc = C.S.N, nc = C.S.n;
     GRID_LOOP(c, nc) {
         int f, I, J;
-        cell_fij(c, Nc, f, I, J);
+        cell_fij(C.S, c, f, I, J);
         const bool inner = I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc;
         const int k0 = F.rstart[c];
         for (int q = 0; q < 16; q++) rw16[q * nc + c] = inner ? F.rw[k0 + q] : 0.f;
@@ -904,7 +904,7 @@ __global__ void k_check_structured(LevelDev F, LevelDev C, int *bad) {
     const int Nf = F.S.N, Nc = C.S.N;
     GRID_LOOP(c, C.S.n) {
         int f, I, J;
-        cell_fij(c, Nc, f, I, J);
+        cell_fij(C.S, c, f, I, J);
         if (!(I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc)) continue;
         int k0 = F.rstart[c], k1 = F.rstart[c + 1];
         if (k1 - k0 != 16) {
@@ -921,7 +921,7 @@ __global__ void k_check_structured(LevelDev F, LevelDev C, int *bad) {
     }
     GRID_LOOP(i, F.S.n) {
         int f, fi, fj;
-        cell_fij(i, Nf, f, fi, fj);
+        cell_fij(F.S, i, f, fi, fj);
         const int I0 = (fi - 1) >> 1, J0 = (fj - 1) >> 1;
         if (!(I0 >= 0 && J0 >= 0 && I0 + 1 < Nc && J0 + 1 < Nc)) continue;
         const int t0 = (f * Nc + J0) * Nc + I0;
