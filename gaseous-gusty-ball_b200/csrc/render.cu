@@ -492,6 +492,7 @@ constexpr int kRec = 768;      // records of one window (shared memory)
 constexpr int kEnt = 2304;     // (record, texel) entries of one window
 constexpr int kHist = 1024;    // key buckets when a dense tile is cut into windows
 constexpr int kBucket = 16;    // entry slots per texel of the one-pass path
+constexpr int kBucketStride = 18;  // slots between texels: 9 words, so a warp's texels hit distinct banks
 
 struct TileSmem {
     union {
@@ -505,7 +506,7 @@ struct TileSmem {
     unsigned short box[kRec];
     union {
         unsigned short ent[kEnt];                 // entry lists packed by a count scan
-        unsigned short bucket[kT * kT * kBucket];  // kBucket entry slots per texel (one-pass path)
+        unsigned short bucket[kT * kT * kBucketStride];  // kBucket entry slots per texel (one-pass path)
     };
     int cnt[kT * kT];
     int start[kT * kT];
@@ -809,7 +810,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
                 box_texels(box, [&](int t) {
                     const int k = atomicAdd(&S.cnt[t], 1);
                     if (k < kBucket)
-                        S.bucket[t * kBucket + k] = (unsigned short)s;
+                        S.bucket[t * kBucketStride + k] = (unsigned short)s;
                     else
                         S.full = 1;
                 });
@@ -822,7 +823,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
         __syncthreads();
         if (m <= kRec && !S.full) {
             const int c = S.cnt[q];
-            if (c) blend_texel(S, S.bucket + q * kBucket, c, q, C, G, d);
+            if (c) blend_texel(S, S.bucket + q * kBucketStride, c, q, C, G, d);
         } else if (m <= kRec && S.tot <= kEnt) {
             // a texel with more than kBucket entries: pack the lists by a count scan
             const int c = S.cnt[q];
