@@ -262,6 +262,13 @@ def run_ours(a, rank, world, local):
     for _ in range(max(3, a.warmup)):
         pl.step()
     K = a.steps
+    # the output path's one-time set-up (its device scratch) belongs to the
+    # warm-up, like the steps' own: one encode to pinned host memory here
+    R = CFG["R"]
+    face_bytes = 6 * R * R * 4
+    host_faces = torch.empty(face_bytes, dtype=torch.uint8).pin_memory().numpy()
+    host_ptr = host_faces.ctypes.data_as(C.POINTER(C.c_ubyte))
+    api.lib.ggb_encode_faces(C.byref(pl.sp.r), None, None, host_ptr)
 
     # The per-step cost drifts as the flow evolves (the splat's sample count
     # follows the speed distribution), so the e2e loop below replays the same K
@@ -298,10 +305,6 @@ def run_ours(a, rank, world, local):
     # ---- e2e: same loop plus the driver's output step at its cadence: the six
     # faces as transparent 8-bit RGBA images (upstream write_outputs' default),
     # encoded on the GPU and copied to pinned host memory
-    R = CFG["R"]
-    face_bytes = 6 * R * R * 4
-    host_faces = torch.empty(face_bytes, dtype=torch.uint8).pin_memory().numpy()
-    host_ptr = host_faces.ctypes.data_as(C.POINTER(C.c_ubyte))
     every = CFG["every"]
     # three runs of the loop, each from the checkpoint; the median is reported
     # (a single host stall of the wall clock would otherwise move the figure)
