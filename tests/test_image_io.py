@@ -156,3 +156,19 @@ def test_save_errors_leave_no_file(io, tmp_path, capfd):
     assert io.save(str(tmp_path / "nodir" / "x.png"), np.zeros((2, 2, 3), np.uint8)) == -1
     err = capfd.readouterr().err
     assert err.count("x.png: ") == 3
+
+
+def test_strip_written_as_the_driver_input(tmp_path):
+    """`python ggb_inputs.py OUT.png [seed]` writes the seeded benchmark strip
+    as an 8-bit RGBA PNG equal to ggb_inputs.strip() rounded to bytes."""
+    import subprocess
+    import sys
+
+    import ggb_inputs
+    f = tmp_path / "strip.png"
+    script = os.path.join(os.path.dirname(ggb_api.__file__), "ggb_inputs.py")
+    p = subprocess.run([sys.executable, script, str(f), "3"], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    got, _ = pngfile.decode(f.read_bytes())
+    want = np.round(ggb_inputs.strip(3) * 255).astype(np.uint8)
+    np.testing.assert_array_equal(got, want)
