@@ -58,6 +58,9 @@ def args_():
     p.add_argument("--workload", choices=["default", "large", "batch"], default="default",
                    help="large: N=512, 4M particles, 2048^2 faces, forcing 0.5, rotation 10; "
                         "batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping")
+    p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
+                   help="plain: FP32 solve with FP64 stencil sums; mixed: FP16 V-cycle storage, FP32 accumulation, "
+                        "flexible CG (FP64 dots and mean projections in both)")
     p.add_argument("--cells-per-block", type=int, default=0,
                    help="batch: cells per block of the batched solves (0: tune over a few candidates)")
     return p.parse_args()
@@ -76,9 +79,11 @@ def working_set_note(cfg):
 
 
 class Planet:
-    """One planet (grid, fluid, particles, faces) of a library."""
+    """One planet (grid, fluid, particles, faces) of a library.  The initial
+    velocity comes from vel_fn (the library's initial condition) or, when
+    given, from the arrays vel0 / vband0."""
 
-    def __init__(self, api, cfg, seed, vel_fn):
+    def __init__(self, api, cfg, seed, vel_fn, mixed=False, vel0=None, vband0=None):
         self.api, self.cfg = api, cfg
         self.g = api.grid(cfg["N"])
         ip = G.InitParams(cfg["bands"], cfg["band_amp"], cfg["noise_amp"], cfg["noise_scale"],
@@ -86,20 +91,27 @@ class Planet:
         n = self.g.n
         vel = np.zeros(3 * n, api.np_real)
         vb = np.zeros(3 * n, api.np_real)
-        vel_fn(C.byref(self.g.cs), C.byref(ip), api.ptr(vel), api.ptr(vb))
+        if vel0 is None:
+            vel_fn(C.byref(self.g.cs), C.byref(ip), api.ptr(vel), api.ptr(vb))
+        else:
+            vel[:] = vel0
+            vb[:] = vband0
+        self.vel0, self.vband0 = vel, vb
         self.fs = G.FluidSim(api, self.g, forcing=cfg["forcing"], rotation=cfg["rotation"], cg_tol=cfg["cg_tol"],
-                             cg_maxit=cfg["cg_maxit"])
+                             cg_maxit=cfg["cg_maxit"], mixed=mixed)
         self.fs.set_state(vel, vb if cfg["forcing"] > 0 else None)
         self.ps = G.ParticleSet(api, cfg["particles"])
         self.ps.colour(ggb_inputs.strip(seed))
         self.sp = G.Splat(api, cfg["R"], cfg["radius"], cfg["alpha"])
         self.h = self.g.cs.h
 
-    def step(self):
-        """upstream src/main.c:422-434"""
+    def step(self, dt=None):
+        """upstream src/main.c:422-434 (dt given: that time step instead of the CFL step)"""
         lib, cfg = self.api.lib, self.cfg
-        vmax = lib.fluid_max_speed(C.byref(self.fs.F))
-        dt = cfg["cfl"] * self.h / (vmax if vmax > 1e-6 else 1e-6)
+        if dt is None:
+            vmax = lib.fluid_max_speed(C.byref(self.fs.F))
+            dt = cfg["cfl"] * self.h / (vmax if vmax > 1e-6 else 1e-6)
+        self.last_dt = dt
         lib.particles_advect(C.byref(self.ps.P), C.byref(self.g.cs), self.fs.F.vel, dt)
         lib.fluid_step(C.byref(self.fs.F), dt)
         lib.render_fade(C.byref(self.sp.r), cfg["fade"])
@@ -164,25 +176,97 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(steps, threads=None):
-    """The upstream CPU implementation on this host: `steps` steps of the workload."""
-    path = os.path.join(ROOT, "oracle", "_ref", "libggbref64.so")
-    if not os.path.exists(path):
-        return None
-    ref = G.Api(path, C.c_double)
-    nthreads = threads or os.cpu_count()
-    ref.lib.drv_set_threads(nthreads)
-    pl = Planet(ref, CFG, CFG["seed"], ref.lib.drv_initial_velocity)
-    pl.step()  # warm-up
+def host_cores():
+    """(physical cores, logical CPUs) of this host, from lscpu where available."""
+    logical = os.cpu_count()
+    try:
+        out = subprocess.run(["lscpu", "-p=CORE,SOCKET"], capture_output=True, text=True, timeout=10).stdout
+        phys = len({ln.strip() for ln in out.splitlines() if ln.strip() and not ln.startswith("#")})
+    except (OSError, subprocess.SubprocessError):
+        phys = None
+    return phys or None, logical
+
+
+def _time_ref(path, real, cfg, steps, threads, warm=1):
+    ref = G.Api(path, real)
+    ref.lib.drv_set_threads(threads)
+    pl = Planet(ref, cfg, cfg["seed"], ref.lib.drv_initial_velocity)
+    for _ in range(warm):
+        pl.step()
     t0 = time.perf_counter()
     its = [pl.step() for _ in range(steps)]
     dt = time.perf_counter() - t0
+    return pl, dt, its
+
+
+def fp64_error(ref_pl, dts, cfg, mixed):
+    """psi / u / particle error of the CUDA path against the FP64 upstream
+    build after the same steps from the same initial state and time steps."""
+    api = G.Api(G.PRODUCT_LIB, C.c_float)
+    gp = Planet(api, cfg, cfg["seed"], None, mixed=mixed, vel0=ref_pl.vel0.astype(np.float32),
+                vband0=ref_pl.vband0.astype(np.float32))
+    for dt in dts:
+        gp.step(dt)
+    f64 = ref_pl.fs
+    n = gp.g.n
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+    p_g = gp.ps.array("pos", 3).astype(np.float64)
+    p_r = ref_pl.ps.array("pos", 3)
+    cosang = np.sum(p_g * p_r, 1) / np.linalg.norm(p_g, axis=1) / np.linalg.norm(p_r, axis=1)
+    ang = np.arccos(np.clip(cosang, -1, 1))
+    out = {"steps": len(dts), "psi_rel_l2": rel(gp.fs.field("psi"), f64.field("psi")),
+           "u_rel_l2": rel(gp.fs.field("vel", 3), f64.field("vel", 3)),
+           "omega_rel_l2": rel(gp.fs.field("omega"), f64.field("omega")),
+           "particle_angle_median_rad": float(np.median(ang)), "particle_angle_p99_rad": float(np.percentile(ang, 99)),
+           "reference": f"upstream sources built with -Dfloat=double, PCG tolerance {cfg['cg_tol']:g} (same as the "
+                        f"GPU path), same initial velocity and time steps; cells {n}"}
+    gp.free()
+    return out
+
+
+def cpu_baseline(steps, mixed=False):
+    """The upstream CPU implementation on this host: `steps` steps of the
+    workload (FP64 build: the FP32 build diverges at PCG tolerance 1e-6), plus
+    the legs of the baseline plan on the FP32 build at upstream's default PCG
+    tolerance 1e-4 (the small workload, and this workload), and the CUDA path's
+    error against the FP64 build after the same steps."""
+    path64 = os.path.join(ROOT, "oracle", "_ref", "libggbref64.so")
+    path32 = os.path.join(ROOT, "oracle", "_ref", "libggbref32.so")
+    if not os.path.exists(path64):
+        return None
+    phys, logical = host_cores()
+    nthreads = logical
+    pl, dt, its = _time_ref(path64, C.c_double, CFG, steps, nthreads)
+    dts = []
+    # the FP64 reference's time steps (the warm-up step, then the timed ones) for the error comparison
+    out = dict(value=steps / dt, unit="steps/s", cores=nthreads, physical_cores=phys, logical_cpus=logical,
+               kind="reference",
+               sample=f"{steps} steps of the same workload after 1 warm-up step, upstream sources compiled "
+                      f"unmodified with -O3 -fopenmp and -Dfloat=double (the FP32 build diverges at PCG "
+                      f"tolerance {CFG['cg_tol']:g}), {nthreads} OpenMP threads; mean CG its {np.mean(its):.1f}",
+               ms_per_step=1000 * dt / steps)
     pl.free()
-    return dict(value=steps / dt, unit="steps/s", cores=nthreads, kind="reference",
-                sample=f"{steps} steps of the same workload after 1 warm-up step, upstream sources compiled "
-                       f"unmodified with -O3 -fopenmp and -Dfloat=double (the FP32 build diverges at PCG "
-                       f"tolerance 1e-6), {nthreads} OpenMP threads; mean CG its {np.mean(its):.1f}",
-                ms_per_step=1000 * dt / steps)
+    # FP64 error of the CUDA path: a fresh FP64 planet, a few steps, the same steps on the GPU
+    ref = G.Api(path64, C.c_double)
+    ref.lib.drv_set_threads(nthreads)
+    rp = Planet(ref, CFG, CFG["seed"], ref.lib.drv_initial_velocity)
+    for _ in range(3):
+        rp.step()
+        dts.append(rp.last_dt)
+    out["fp64_error"] = fp64_error(rp, dts, CFG, mixed)
+    rp.free()
+    legs = []
+    if os.path.exists(path32):
+        for name, cfg, k in (("small workload: N=64, 100k particles, 256^2 faces (FP32 build, PCG tol 1e-4)",
+                              ggb_inputs.SMALL, 40),
+                             (f"this workload at PCG tol 1e-4 (FP32 build, upstream's default tolerance)",
+                              dict(CFG, cg_tol=1e-4), 5)):
+            p32, d32, i32 = _time_ref(path32, C.c_float, cfg, k, nthreads)
+            p32.free()
+            legs.append({"workload": name, "value": k / d32, "unit": "steps/s", "ms_per_step": 1000 * d32 / k,
+                         "steps": k, "threads": nthreads, "mean_cg_iters": float(np.mean(i32))})
+    out["legs"] = legs
+    return out
 
 
 # ---------------------------------------------------------------- arms
@@ -258,7 +342,8 @@ def run_ours(a, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    pl = Planet(api, CFG, CFG["seed"] + rank, api.lib.ggb_initial_velocity)
+    mixed = a.precision == "mixed"
+    pl = Planet(api, CFG, CFG["seed"] + rank, api.lib.ggb_initial_velocity, mixed=mixed)
     for _ in range(max(3, a.warmup)):
         pl.step()
     K = a.steps
@@ -359,14 +444,18 @@ def run_ours(a, rank, world, local):
 
     base = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        base = cpu_baseline(steps=5)
+        base = cpu_baseline(steps=5, mixed=mixed)
 
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K, "warmup": a.warmup,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f16" if mixed else "f32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world} (one planet per GPU)",
+                       "precision": ("mixed: FP16 V-cycle vectors and coarse slot weights, FP32 accumulation, "
+                                     "flexible FP32 CG, FP64 dots / norms / mean projections") if mixed else
+                                    "plain: FP32 vectors, FP64 stencil sums, FP64 dots / norms / mean projections",
                        "l2": working_set_note(CFG),
                        "mean_cg_iters": kit,
                        "deposit_repeats": int(api.lib.ggb_render_repeats(C.byref(pl.sp.r))),

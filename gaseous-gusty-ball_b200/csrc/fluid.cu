@@ -289,6 +289,12 @@ __global__ void k_rsort(int nc, const int *rstart, int *rkey, const float *pw, i
     }
 }
 
+// FP16 copy of a level's slot weights (mixed-precision V-cycle).
+__global__ void k_to_half(size_t n, const float *src, __half *dst) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = __float2half_rn(src[i]);
+}
+
 // ------------------------------------------------------------ private state
 
 struct FluidPriv {
@@ -311,6 +317,13 @@ struct FluidPriv {
     float *rw16[kMaxLev] = {};     // coarse-major structured restriction weights
     double *dense = nullptr;       // dense map of the V-cycle below the grid levels
     int nd = 0;
+    int last_flags = 0;            // kSolve* bits of the last solve
+    // mixed-precision solve (ggb_fluid_set_precision): FP16 level vectors,
+    // FP16 slot weights of the coarse levels, the previous z
+    int mixed = 0;
+    __half *hx[kMaxLev] = {}, *hxo[kMaxLev] = {}, *hb[kMaxLev] = {}, *hr[kMaxLev] = {};
+    __half *wh[kMaxLev] = {};
+    float *z2 = nullptr;
 };
 
 static FluidPriv *priv_of(const Fluid *F) {
@@ -320,6 +333,7 @@ static FluidPriv *priv_of(const Fluid *F) {
 
 static StencilDev stencil_of(const GridTables *t) {
     StencilDev s;
+    s.wslot_h = nullptr;
     s.N = t->N;
     s.n = t->n;
     s.nring = t->nring;
@@ -404,10 +418,18 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
         LevelDev &L = P.L[l];
         L.S = stencil_of(t);
         L.dinv = t->dinv;
-        L.x = Pv->lx[l] ? Pv->lx[l] : nullptr;
-        L.xo = Pv->lxo[l];
-        L.b = Pv->lb[l];
-        L.r = Pv->lr[l];
+        if (Pv->mixed) {
+            L.S.wslot_h = Pv->wh[l];
+            L.x = Pv->hx[l];
+            L.xo = Pv->hxo[l];
+            L.b = Pv->hb[l];
+            L.r = Pv->hr[l];
+        } else {
+            L.x = Pv->lx[l];
+            L.xo = Pv->lxo[l];
+            L.b = Pv->lb[l];
+            L.r = Pv->lr[l];
+        }
         if (l + 1 < Pv->nlev) {
             L.ptap = Pv->ptap[l];
             L.pw = Pv->pw[l];
@@ -437,6 +459,8 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
     P.p2 = Pv->p2;
     P.Ap = F->Ap;
     P.z = F->z;
+    P.mixed = Pv->mixed;
+    P.z2 = Pv->z2;
     P.part = Pv->part;
     P.bar = Pv->bar;
     P.res = Pv->res;
@@ -450,6 +474,7 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
 // Structured-transfer flags and the dense coarse map (after build_levels).
 static void finish_levels(Fluid *F, FluidPriv *Pv) {
     SolveParams P = solve_params(F, Pv, 0, 1);
+    P.mixed = 0;
     for (int l = 0; l + 1 < Pv->nlev; l++) {
         LevelDev Fl = P.L[l], C = P.L[l + 1];
         Fl.structured = 0;
@@ -483,6 +508,7 @@ static void solve_launch(Fluid *F, FluidPriv *Pv, int remove_mean, int maxit, in
 
 static int solve_collect(Fluid *F, FluidPriv *Pv) {
     const SolveResult &R = *Pv->res_host;
+    Pv->last_flags = R.flags;
     if (R.status != 0) fail_msg("Poisson solve aborted: a grid barrier timed out");
     F->cg_iters = R.iters;
     F->cg_relres = R.relres;
@@ -615,7 +641,13 @@ GGB_EXPORT void fluid_free(Fluid *F) {
         dev_free(Pv->lxo[l]);
         dev_free(Pv->lb[l]);
         dev_free(Pv->lr[l]);
+        dev_free(Pv->hx[l]);
+        dev_free(Pv->hxo[l]);
+        dev_free(Pv->hb[l]);
+        dev_free(Pv->hr[l]);
+        dev_free(Pv->wh[l]);
     }
+    dev_free(Pv->z2);
     dev_free(Pv->r2);
     dev_free(Pv->p2);
     dev_free(Pv->part);
@@ -628,6 +660,46 @@ GGB_EXPORT void fluid_free(Fluid *F) {
     cudaFreeHost(Pv->vmax_host);
     delete Pv;
     memset(F, 0, sizeof(*F));
+}
+
+// Status bits of the last solve of F (kSolve* in ggb_solver.h; see ggb_ext.h).
+GGB_EXPORT int ggb_solve_flags(const Fluid *F) { return priv_of(F)->last_flags; }
+
+// Switches the Poisson solve of F between the plain form (mixed = 0: FP32
+// vectors, FP64 stencil accumulation, the upstream CG) and the mixed-precision
+// form (mixed = 1: FP16 V-cycle vectors and coarse slot weights, FP32
+// accumulation, flexible CG).  The buffers of the mixed form are allocated on
+// the first switch.  Returns 0, or -1 for a fluid without multigrid.
+GGB_EXPORT int ggb_fluid_set_precision(Fluid *F, int mixed) {
+    FluidPriv *Pv = priv_of(F);
+    if (!mixed) {
+        Pv->mixed = 0;
+        return 0;
+    }
+    if (!F->prm.multigrid || Pv->nlev < 1) {
+        fprintf(stderr, "ggb_fluid_set_precision: the mixed-precision solve needs the multigrid preconditioner\n");
+        return -1;
+    }
+    if (!Pv->z2) {
+        cudaStream_t s = stream();
+        for (int l = 0; l < Pv->nlev; l++) {
+            const GridTables *t = l == 0 ? Pv->grid0 : &Pv->coarse[l];
+            const size_t n = t->n;
+            Pv->hx[l] = (__half *)dev_alloc(sizeof(__half) * n);
+            Pv->hxo[l] = (__half *)dev_alloc(sizeof(__half) * n);
+            Pv->hb[l] = (__half *)dev_alloc(sizeof(__half) * n);
+            Pv->hr[l] = (__half *)dev_alloc(sizeof(__half) * n);
+            if (l >= 1) {
+                Pv->wh[l] = (__half *)dev_alloc(sizeof(__half) * 4 * n);
+                k_to_half<<<blocks_for((int)std::min<size_t>(4 * n, 1u << 30)), kB, 0, s>>>(4 * n, t->wslot, Pv->wh[l]);
+                GGB_LAUNCHED();
+            }
+        }
+        Pv->z2 = (float *)dev_alloc(sizeof(float) * F->cs->ncells);
+        sync();
+    }
+    Pv->mixed = 1;
+    return 0;
 }
 
 GGB_EXPORT int fluid_solve_psi(Fluid *F) {

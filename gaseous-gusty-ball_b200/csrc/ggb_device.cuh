@@ -240,15 +240,16 @@ __device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, un
     return old;
 }
 
-// Returns true when all blocks arrived; false on timeout or an error raised
-// by another block.  `count` counts arrivals since the launch began (the host
-// zeroes it before every launch): thread 0 arrives with one acq_rel atomic
+// Returns true when all blocks arrived; false on timeout (limit_ns after the
+// first 64 polls) or an error raised by another block.  `count` counts
+// arrivals since the launch began (the host zeroes it before every launch):
+// thread 0 arrives with one acq_rel atomic
 // after a block barrier (so every write of the block before the barrier is
 // released), and the barrier is complete when the count reaches the next
 // multiple of the number of blocks, which the waiters poll with acquire loads.
 // The arrival is the first global access of a barrier (no generation or error
 // read before it); the error flag and the timeout are checked every 64 polls.
-__device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
+__device__ __forceinline__ bool grid_sync_limit(GridBarrier *bar, unsigned long long limit_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -267,7 +268,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
                 const unsigned long long t = globaltimer_ns();
                 if (polls == 64u) {
                     t0 = t;
-                } else if (t - t0 > kBarrierTimeoutNs) {
+                } else if (t - t0 > limit_ns) {
                     atomicExch(&bar->err, 1);
                     ok = 0;
                     break;
@@ -279,6 +280,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *bar) {
     __syncthreads();
     return s_ok != 0;
 }
+__device__ __forceinline__ bool grid_sync(GridBarrier *bar) { return grid_sync_limit(bar, kBarrierTimeoutNs); }
 
 // ------------------------------------------------------------ reductions
 // Block sum of one double per thread, returned to every thread.  The

@@ -41,6 +41,8 @@ long launch_count();
 // The stream every entry point issues its work on; created on first use for
 // the current device.  The batched API may redirect it while capturing.
 cudaStream_t stream();
+// The device the library's own stream was created on (-1 before the first stream()).
+int stream_device();
 void set_stream(cudaStream_t s);
 void sync();
 int device_sm_count();
@@ -67,9 +69,13 @@ void particles_advect_queue(Particles *P, const CubeSphere *cs, const float *vel
 void render_pending_get(const Render *r, int *pending, float *scale);
 void render_pending_set(Render *r, int pending, float scale);
 
-void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled
+void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled; exits on failure
 void dev_free(void *p);
-void *managed_alloc(size_t bytes);  // cudaMallocManaged, zero-filled, resident on the device
+void *managed_alloc(size_t bytes);  // cudaMallocManaged, zero-filled, resident on the device; exits on failure
+// The same, returning nullptr when the allocation fails (for entry points
+// that report failure with -1, as upstream's *_init do).
+void *dev_try_alloc(size_t bytes);
+void *managed_try_alloc(size_t bytes);
 void managed_free(void *p);
 
 inline unsigned grid_for(size_t n, int block) { return (unsigned)((n + block - 1) / block); }
@@ -83,6 +89,7 @@ inline unsigned grid_for(size_t n, int block) { return (unsigned)((n + block - 1
 //       face (or the 3x3 box); -1 terminates.  Only ring cells have such links.
 struct GridTables {
     int N = 0, n = 0, nring = 0;
+    int device = -1;  // the CUDA device the tables live on
     double h = 0;
     bool managed = false;
     // upstream layout (managed memory for a public grid, device memory otherwise)
@@ -119,6 +126,7 @@ void grid_release(GridTables *t);
 
 // Registry: the private tables of a public CubeSphere, keyed by cs->pos.
 GridTables *grid_lookup(const CubeSphere *cs);  // fails loudly when unknown
+GridTables *grid_find(const CubeSphere *cs);    // nullptr when unknown
 
 // Device copy of an argument that may live in pageable host memory: returns
 // a device-accessible pointer to `bytes` bytes equal to `src` (staging it

@@ -7,14 +7,15 @@ namespace ggb {
 
 constexpr int kMaxLev = 12;
 
-// One multigrid level on the device.
+// One multigrid level on the device.  The level vectors are float in the
+// plain solve and __half in the mixed-precision solve (SolveParams::mixed).
 struct LevelDev {
     StencilDev S;
     const float *dinv;  // [n] 1 / sum of link weights
-    float *x;           // [n] iterate (pre-smoothed, then corrected)
-    float *xo;          // [n] V-cycle output of this level
-    float *b;           // [n] right-hand side (restricted residual)
-    float *r;           // [n] residual after the pre-smooth
+    void *x;            // [n] iterate (pre-smoothed, then corrected)
+    void *xo;           // [n] V-cycle output of this level
+    void *b;            // [n] right-hand side (restricted residual)
+    void *r;            // [n] residual after the pre-smooth
     // transfer to the next coarser level
     const int *ptap;    // [4n] coarse taps of each cell of this level
     const float *pw;    // [4n] their bilinear weights
@@ -25,15 +26,25 @@ struct LevelDev {
     const float *rw16;  // [16][n_coarse] weights of the structured R rows (coarse-major), or nullptr
 };
 
+// Status bits of a solve (SolveResult::flags; also ggb_solve_flags).
+enum {
+    kSolveTimeout = 1,    // a grid barrier timed out (the solve was abandoned)
+    kSolveNonFinite = 2,  // a NaN or Inf reached b.b, r.r, r.z or p.Ap
+    kSolveBreakdown = 4,  // p.Ap <= 0: CG stopped early (upstream src/fluid.c:329-330 stops silently)
+    kSolveMaxit = 8,      // maxit iterations without reaching the tolerance
+};
+
 struct SolveResult {
     int iters;
     int status;      // 0 ok, 1 barrier timeout
     double relres;
     int r_final;     // which r buffer holds the final residual (0: r, 1: r2)
-    int pad;
+    int flags;       // kSolve* bits
 };
 
 struct SolveParams {
+    int mixed;           // 1: V-cycle vectors (and coarse slot weights) in FP16 with FP32 accumulation,
+                         //    flexible (Polak-Ribiere) CG; 0: FP32 vectors, FP64 accumulation
     int nlev;            // >= 1 when multigrid, 0 for the Jacobi preconditioner
     int nlev_grid;       // non-coarsest levels 0..nlev_grid-1 run grid-wide
     int coarse_on_grid;  // coarsest level swept grid-wide (else by block 0)
@@ -46,6 +57,7 @@ struct SolveParams {
     const float *area;   // level-0 cell areas
     float *omega, *psi;
     float *r, *r2, *p, *p2, *Ap, *z;  // level-0 CG vectors (r / p ping-pong)
+    float *z2;           // mixed: the previous z (z / z2 ping-pong for the flexible beta)
     double *part;        // [RED_N][gridDim.x] per-block partial sums
     unsigned long long *trace;  // optional: block 0 stamps %globaltimer at phase marks
     int trace_cap;

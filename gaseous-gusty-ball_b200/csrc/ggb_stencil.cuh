@@ -4,6 +4,8 @@
 // on the fly from other vectors).
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "ggb_device.cuh"
 
 namespace ggb {
@@ -13,6 +15,7 @@ struct StencilDev {
     int lgN;              // log2(N) when N is a power of two, else -1
     const float *wslot;   // [4][n]: E, N, NE, NW weights (0 = no link)
     const double *wslot_d;  // the same in FP64
+    const __half *wslot_h;  // the same in FP16 (mixed-precision V-cycle, levels >= 1), or nullptr
     const int *ring_nb;   // [6*nring][8], -1 terminated
     const float *ring_w;  // [6*nring][8]
 };
@@ -141,13 +144,13 @@ __device__ __forceinline__ void ring_cell_of_rank(int R, int N, int nring, int &
 // (also where the neighbouring index wraps to another row or face), so its
 // term adds an exact zero.  A boundary-ring cell adds the staged sum of its
 // links that leave the face, rsum[ring rank - r0].
-__device__ __forceinline__ double apply_k_smem(const StencilDev &S, int c, double xc, const double *x,
-                                               const double *wE, const double *wN, const double *wNE,
-                                               const double *wNW, const double *rsum, int r0) {
+template <class A>
+__device__ __forceinline__ A apply_k_smem(const StencilDev &S, int c, A xc, const A *x, const A *wE, const A *wN,
+                                          const A *wNE, const A *wNW, const A *rsum, int r0) {
     const int N = S.N;
     int f, i, j;
     cell_fij(S, c, f, i, j);
-    double s = wE[c] * (xc - x[c + 1]);
+    A s = wE[c] * (xc - x[c + 1]);
     s += wN[c] * (xc - x[c + N]);
     s += wNE[c] * (xc - x[c + N + 1]);
     s += wNW[c] * (xc - x[c + N - 1]);

@@ -347,7 +347,7 @@ __global__ void k_sum_area(int n, const double *a, double *out) {
     if (threadIdx.x == 0) *out = t;
 }
 
-static void *talloc(bool managed, size_t bytes) { return managed ? managed_alloc(bytes) : dev_alloc(bytes); }
+static void *talloc(bool managed, size_t bytes) { return managed ? managed_try_alloc(bytes) : dev_try_alloc(bytes); }
 static void tfree(bool managed, void *p) {
     if (managed)
         managed_free(p);
@@ -366,6 +366,7 @@ int grid_build(GridTables *t, int N, bool managed) {
     }
     cudaStream_t s = stream();
     int n = 6 * N * N;
+    GGB_CHECK(cudaGetDevice(&t->device));
     t->N = N;
     t->n = n;
     t->h = (kPi / 2) / N;
@@ -378,17 +379,30 @@ int grid_build(GridTables *t, int N, bool managed) {
     t->w = (float *)talloc(managed, sizeof(float) * kMaxNb * n);
     t->elen = (float *)talloc(managed, sizeof(float) * kMaxNb * n);
     t->gc = (float *)talloc(managed, sizeof(float) * 3 * kMaxNb * n);
-    t->ghost = (int *)dev_alloc(sizeof(int) * 6 * (4 * N + 4));
-    t->wslot = (float *)dev_alloc(sizeof(float) * 4 * n);
-    t->wslot_d = (double *)dev_alloc(sizeof(double) * 4 * n);
-    t->ring_nb = (int *)dev_alloc(sizeof(int) * kMaxNb * 6 * t->nring);
-    t->ring_w = (float *)dev_alloc(sizeof(float) * kMaxNb * 6 * t->nring);
-    t->dinv = (float *)dev_alloc(sizeof(float) * n);
-    float *rawlen = (float *)dev_alloc(sizeof(float) * kMaxNb * n);
-    float *symlen = (float *)dev_alloc(sizeof(float) * kMaxNb * n);
-    double *area64 = (double *)dev_alloc(sizeof(double) * n);
-    int *counters = (int *)dev_alloc(sizeof(int) * 4);
-    double *tot = (double *)dev_alloc(sizeof(double));
+    t->ghost = (int *)dev_try_alloc(sizeof(int) * 6 * (4 * N + 4));
+    t->wslot = (float *)dev_try_alloc(sizeof(float) * 4 * n);
+    t->wslot_d = (double *)dev_try_alloc(sizeof(double) * 4 * n);
+    t->ring_nb = (int *)dev_try_alloc(sizeof(int) * kMaxNb * 6 * t->nring);
+    t->ring_w = (float *)dev_try_alloc(sizeof(float) * kMaxNb * 6 * t->nring);
+    t->dinv = (float *)dev_try_alloc(sizeof(float) * n);
+    float *rawlen = (float *)dev_try_alloc(sizeof(float) * kMaxNb * n);
+    float *symlen = (float *)dev_try_alloc(sizeof(float) * kMaxNb * n);
+    double *area64 = (double *)dev_try_alloc(sizeof(double) * n);
+    int *counters = (int *)dev_try_alloc(sizeof(int) * 4);
+    double *tot = (double *)dev_try_alloc(sizeof(double));
+    const void *all[] = {t->pos,   t->area,    t->nnb,   t->nbr,    t->w,    t->elen,   t->gc,     t->ghost, t->wslot,
+                         t->wslot_d, t->ring_nb, t->ring_w, t->dinv, rawlen, symlen, area64, counters, tot};
+    for (const void *q : all)
+        if (!q) {
+            fprintf(stderr, "cs_init: N=%d: device memory allocation failed\n", N);
+            dev_free(rawlen);
+            dev_free(symlen);
+            dev_free(area64);
+            dev_free(counters);
+            dev_free(tot);
+            grid_release(t);
+            return -1;
+        }
 
     unsigned gb = std::min<unsigned>(grid_for(n, kBlk), 148u * 64u);
     k_positions<<<gb, kBlk, 0, s>>>(N, t->h, t->pos);
@@ -450,11 +464,18 @@ void grid_release(GridTables *t) {
 static std::mutex g_reg_mu;
 static std::vector<GridTables *> g_reg;
 
-GridTables *grid_lookup(const CubeSphere *cs) {
+GridTables *grid_find(const CubeSphere *cs) {
+    if (!cs) return nullptr;
     std::lock_guard<std::mutex> lk(g_reg_mu);
     for (GridTables *t : g_reg)
         if (t->pos == cs->pos && cs->pos) return t;
-    fail_msg("grid %p (N=%d) was not created by this library's cs_init", (const void *)cs, cs ? cs->N : -1);
+    return nullptr;
+}
+
+GridTables *grid_lookup(const CubeSphere *cs) {
+    GridTables *t = grid_find(cs);
+    if (!t) fail_msg("grid %p (N=%d) was not created by this library's cs_init", (const void *)cs, cs ? cs->N : -1);
+    return t;
 }
 
 }  // namespace ggb
@@ -590,7 +611,46 @@ __global__ void k_taps_batch(GridDev g, int n, const double *dirs, int *idx, dou
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         taps(g, d3(dirs[3 * k], dirs[3 * k + 1], dirs[3 * k + 2]), idx + 4 * k, wt + 4 * k);
 }
+// Bad entries of the public arrays of a grid (ggb_grid_validate): area,
+// weights and edge lengths must be finite and positive on every link, counts
+// at most kMaxNb, neighbours in range and not the cell itself.
+__global__ void k_validate(int n, const float *area, const unsigned char *nnb, const int *nbr, const float *w,
+                           const float *elen, unsigned long long *bad) {
+    unsigned long long b = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const float a = area[c];
+        b += !(isfinite(a) && a > 0.f);
+        int m = nnb[c];
+        if (m > kMaxNb) {
+            b++;
+            m = kMaxNb;
+        }
+        for (int k = 0; k < m; k++) {
+            const int j = nbr[(size_t)kMaxNb * c + k];
+            const float q = w[(size_t)kMaxNb * c + k], e = elen[(size_t)kMaxNb * c + k];
+            b += (j < 0 || j >= n || j == c);
+            b += !(isfinite(q) && q > 0.f);
+            b += !(isfinite(e) && e > 0.f);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(bad, b);
+}
+
 }  // namespace ggb
+
+GGB_EXPORT long ggb_grid_validate(const CubeSphere *cs) {
+    GridTables *t = grid_lookup(cs);
+    unsigned long long *bad = (unsigned long long *)dev_alloc(sizeof(unsigned long long));
+    k_validate<<<std::max(1u, std::min(grid_for(t->n, 256), 4096u)), 256, 0, stream()>>>(t->n, t->area, t->nnb,
+                                                                                      t->nbr, t->w, t->elen, bad);
+    GGB_LAUNCHED();
+    unsigned long long h = 0;
+    GGB_CHECK(cudaMemcpyAsync(&h, bad, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    sync();
+    dev_free(bad);
+    return (long)h;
+}
 
 // out[k] = cs_cell_of(cs, dirs[k]) computed on the GPU (dirs: n*3 doubles).
 GGB_EXPORT void ggb_cell_of_batch(const CubeSphere *cs, const double *dirs, int n, int *out) {

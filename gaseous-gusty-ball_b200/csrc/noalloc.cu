@@ -83,17 +83,39 @@ static double *scratch_for_current_device() {
 
 using namespace ggb;
 
-// See include/ggb_ext.h.  Returns 0, or -1 (with a message on stderr, f
-// unchanged) when the grid has more than 16,777,216 cells, f is not device or
-// managed memory, or the scratch address cannot be obtained.
+// See include/ggb_ext.h.  Returns 0; or -1 with a message on stderr and f
+// unchanged when the grid is unknown, has more than 16,777,216 cells, lives on
+// another device than the current one or the library stream's, f is not
+// device or managed memory, or the scratch address cannot be obtained; or -1
+// with f undefined when a launch or the final synchronisation fails.
 GGB_EXPORT int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f) {
-    GridTables *t = grid_lookup(cs);
+    GridTables *t = grid_find(cs);
+    if (!t) {
+        fprintf(stderr, "ggb_remove_mean_noalloc: the grid was not created by this library's cs_init\n");
+        return -1;
+    }
     const int n = t->n;
     if ((long)n > kNoAllocMaxCells) {
         fprintf(stderr,
                 "ggb_remove_mean_noalloc: %d cells exceed the fixed scratch of this entry point "
                 "(at most %ld cells, N <= 1672); use fluid_remove_mean\n",
                 n, kNoAllocMaxCells);
+        return -1;
+    }
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        fprintf(stderr, "ggb_remove_mean_noalloc: no current CUDA device\n");
+        return -1;
+    }
+    // the scratch address below is the current device's: the grid's tables and
+    // the library stream must belong to that same device
+    cudaStream_t s = stream();
+    if (t->device != dev || stream_device() != dev) {
+        fprintf(stderr,
+                "ggb_remove_mean_noalloc: the current device (%d) differs from the grid's (%d) or the "
+                "library stream's (%d)\n",
+                dev, t->device, stream_device());
         return -1;
     }
     cudaPointerAttributes a;
@@ -107,13 +129,15 @@ GGB_EXPORT int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f) {
     double *scratch = scratch_for_current_device();
     if (!scratch) return -1;
     const int nb = (n + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock;
-    cudaStream_t s = stream();
     k_noalloc_partials<<<nb, kNoAllocThreads, 0, s>>>(n, t->area, f, scratch);
-    GGB_LAUNCHED();
     k_noalloc_mean<<<1, kNoAllocThreads, 0, s>>>(nb, t->total_area, scratch);
-    GGB_LAUNCHED();
     k_noalloc_subtract<<<nb, kNoAllocThreads, 0, s>>>(n, scratch, f);
-    GGB_LAUNCHED();
-    sync();
+    note_launch(3);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "ggb_remove_mean_noalloc: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
     return 0;
 }

@@ -105,9 +105,17 @@ GGB_EXPORT int particles_init(Particles *P, int n) {
         return -1;
     }
     P->n = n;
-    P->pos = (float *)managed_alloc(sizeof(float) * 3 * (size_t)n);
-    P->prev = (float *)managed_alloc(sizeof(float) * 3 * (size_t)n);
-    P->col = (float *)managed_alloc(sizeof(float) * 4 * (size_t)n);
+    P->pos = (float *)managed_try_alloc(sizeof(float) * 3 * (size_t)n);
+    P->prev = (float *)managed_try_alloc(sizeof(float) * 3 * (size_t)n);
+    P->col = (float *)managed_try_alloc(sizeof(float) * 4 * (size_t)n);
+    if (!P->pos || !P->prev || !P->col) {
+        fprintf(stderr, "particles: device memory allocation failed for %d particles\n", n);
+        managed_free(P->pos);
+        managed_free(P->prev);
+        managed_free(P->col);
+        memset(P, 0, sizeof(*P));
+        return -1;
+    }
     if (n > 0) {
         k_fibonacci<<<blocks_for(n), kPB, 0, stream()>>>(n, P->pos, P->prev, P->col);
         GGB_LAUNCHED();

@@ -1222,7 +1222,12 @@ GGB_EXPORT int render_init(Render *r, int R, float radius, float alpha) {
     r->radius = radius < 0.75f ? 0.75f : radius;
     r->alpha = alpha;
     r->g = 1.0;
-    r->buf = (float *)managed_alloc(sizeof(float) * 6 * (size_t)R * R * 4);
+    r->buf = (float *)managed_try_alloc(sizeof(float) * 6 * (size_t)R * R * 4);
+    if (!r->buf) {
+        fprintf(stderr, "render: device memory allocation failed for 6 faces of %d x %d\n", R, R);
+        memset(r, 0, sizeof(*r));
+        return -1;
+    }
     int sh = 32;
     if (sh < (int)ceilf(r->radius) + 1) sh = (int)ceilf(r->radius) + 1;
     if (sh > R) sh = R;

@@ -34,6 +34,7 @@ long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 static std::mutex g_stream_mu;
 static cudaStream_t g_own_stream = nullptr;
 static cudaStream_t g_override = nullptr;
+static int g_stream_dev = -1;
 static int g_sms = 0;
 
 bool have_device() {
@@ -47,8 +48,14 @@ cudaStream_t stream() {
     if (!g_own_stream) {
         if (!have_device()) fail_msg("no CUDA device is available (this library has no CPU path)");
         GGB_CHECK(cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking));
+        GGB_CHECK(cudaGetDevice(&g_stream_dev));
     }
     return g_own_stream;
+}
+
+int stream_device() {
+    std::lock_guard<std::mutex> lk(g_stream_mu);
+    return g_stream_dev;
 }
 
 void set_stream(cudaStream_t s) { g_override = s; }
@@ -98,11 +105,35 @@ int device_sm_count() {
     return g_sms;
 }
 
-void *dev_alloc(size_t bytes) {
+// Allocation-failure injection (ggb_inject_alloc_failure): while >= 0, the
+// number of allocations that still succeed; the one after fails as if device
+// memory were exhausted, without calling the allocator.
+static std::atomic<long> g_allocs_left{-1};
+
+static bool injected_failure() {
+    long k = g_allocs_left.load();
+    while (k >= 0) {
+        if (k == 0) return true;
+        if (g_allocs_left.compare_exchange_weak(k, k - 1)) return false;
+    }
+    return false;
+}
+
+void *dev_try_alloc(size_t bytes) {
     void *p = nullptr;
     if (!bytes) bytes = 16;
-    GGB_CHECK(cudaMalloc(&p, bytes));
+    if (injected_failure()) return nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
     GGB_CHECK(cudaMemsetAsync(p, 0, bytes, stream()));
+    return p;
+}
+
+void *dev_alloc(size_t bytes) {
+    void *p = dev_try_alloc(bytes);
+    if (!p) fail_msg("device memory allocation of %zu bytes failed", bytes);
     return p;
 }
 
@@ -111,9 +142,19 @@ void dev_free(void *p) {
 }
 
 void *managed_alloc(size_t bytes) {
+    void *p = managed_try_alloc(bytes);
+    if (!p) fail_msg("managed memory allocation of %zu bytes failed", bytes);
+    return p;
+}
+
+void *managed_try_alloc(size_t bytes) {
     void *p = nullptr;
     if (!bytes) bytes = 16;
-    GGB_CHECK(cudaMallocManaged(&p, bytes, cudaMemAttachGlobal));
+    if (injected_failure()) return nullptr;
+    if (cudaMallocManaged(&p, bytes, cudaMemAttachGlobal) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
     int dev = 0;
     GGB_CHECK(cudaGetDevice(&dev));
 #if CUDART_VERSION >= 13000
@@ -181,6 +222,10 @@ void stage_finish(Staged &s) {
 }  // namespace ggb
 
 GGB_EXPORT long ggb_launch_count(void) { return ggb::launch_count(); }
+
+// Host-side fault injection: after `after` more successful allocations every
+// device / managed allocation of the library fails (after < 0: off).
+GGB_EXPORT void ggb_inject_alloc_failure(long after) { ggb::g_allocs_left.store(after < 0 ? -1 : after); }
 
 // Selects the CUDA device this library uses (before any other call).
 GGB_EXPORT int ggb_set_device(int dev) { return cudaSetDevice(dev) == cudaSuccess ? 0 : -1; }

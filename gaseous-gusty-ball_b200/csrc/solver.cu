@@ -5,13 +5,28 @@
 // coarsest grid), with FP64 dot products and FP64 zero-mean projections.
 //
 // Upstream: src/fluid.c:41-160 (multigrid), :264-275 (mean), :290-358 (PCG).
-// The arithmetic of every vector update follows upstream (FP32 vectors, FP64
-// accumulation); the schedule is this library's:
+// Two precisions share one kernel body (template parameter MP):
+//   * plain (MP = false): the arithmetic of every vector update follows
+//     upstream (FP32 vectors, FP64 accumulation of the stencil sums);
+//   * mixed (MP = true): the V-cycle's level vectors and the coarse levels'
+//     slot weights are stored in FP16, every stencil sum, restriction and
+//     prolongation accumulates in FP32, and the outer CG is flexible
+//     (Polak-Ribiere beta = r.(z - z_prev) / rz_prev), which tolerates the
+//     preconditioner's rounding; psi, omega, r, p, z stay FP32 and the dots,
+//     norms and mean projections stay FP64.  FP16 holds about five decimal
+//     orders of magnitude, less than the spread of a residual across the
+//     levels, so the mixed V-cycle runs on scaled vectors: its input is
+//     multiplied by a power of two that brings its RMS near 1/16, restriction
+//     carries a factor 1/4 and prolongation a factor 4 (so that every level's
+//     right-hand side stays at the input's scale instead of growing 4x per
+//     level), and the output is scaled back.  All factors are powers of two
+//     (exact), and the V-cycle is linear, so they change nothing but the range.
+// The schedule is this library's:
 //   * phases are separated by a bounded grid-wide barrier instead of host loops;
 //   * each block owns a contiguous range of cells of every level; a stencil
 //     phase first computes the (transformed) neighbour value of every cell of
-//     the range plus its halo once, in FP64, into shared memory, then applies
-//     the stencil with FP64 weights (no FP32/FP64 conversion per link);
+//     the range plus its halo once into shared memory (FP64 plain, FP32
+//     mixed), then applies the stencil from shared memory;
 //   * p = z + beta p and r - alpha Ap are recomputed inside K p and the level-0
 //     pre-smooth, which saves two barriers per iteration;
 //   * interior rows of R and P use index arithmetic (no CSR indirection);
@@ -20,6 +35,7 @@
 //     blocks from L2.
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "ggb_internal.h"
@@ -34,8 +50,65 @@ constexpr int kStageCap = 3584;     // cells of a block's staged window (value +
 constexpr int kRingCap = 1024;      // boundary-ring cells of one staged sub-range (their off-face link sums)
 constexpr int kStageWords = kStageCap * 5 + (kStageCap * 3 + 1) / 2 + kRingCap;  // in doubles
 constexpr size_t kStageBytes = (size_t)kStageWords * sizeof(double);
+static_assert((kStageCap * 3) % 2 == 0, "the ring sums follow the own-input arrays on an 8-byte boundary");
 
-enum { RED_BB = 0, RED_RR, RED_PAP, RED_RZ, RED_MEAN, RED_AREA, RED_N };
+enum { RED_BB = 0, RED_RR, RED_PAP, RED_RZ, RED_MEAN, RED_AREA, RED_RZO, RED_N };
+
+// Storage (V) and accumulation (A) types of the two precisions.
+template <bool MP>
+struct Prec {
+    using V = float;
+    using A = double;
+};
+template <>
+struct Prec<true> {
+    using V = __half;
+    using A = float;
+};
+
+__device__ __forceinline__ float ldv(const float *p, int k) { return p[k]; }
+__device__ __forceinline__ float ldv(const __half *p, int k) { return __half2float(p[k]); }
+__device__ __forceinline__ void stv(float *p, int k, float v) { p[k] = v; }
+__device__ __forceinline__ void stv(__half *p, int k, float v) { p[k] = __float2half_rn(v); }
+// store and return the stored value
+__device__ __forceinline__ float stv_get(float *p, int k, float v) {
+    p[k] = v;
+    return v;
+}
+__device__ __forceinline__ float stv_get(__half *p, int k, float v) {
+    const __half h = __float2half_rn(v);
+    p[k] = h;
+    return __half2float(h);
+}
+// v as the storage type would hold it (rounded to FP16 in the mixed solve)
+template <bool MP>
+__device__ __forceinline__ float as_stored(float v) {
+    return MP ? __half2float(__float2half_rn(v)) : v;
+}
+template <bool MP>
+__device__ __forceinline__ typename Prec<MP>::V *lv(void *p) {
+    return static_cast<typename Prec<MP>::V *>(p);
+}
+
+// Scale factors of the mixed V-cycle's transfers (1 in the plain solve).
+template <bool MP>
+__device__ __forceinline__ float restrict_scale() {
+    return MP ? 0.25f : 1.0f;
+}
+template <bool MP>
+__device__ __forceinline__ float prolong_scale() {
+    return MP ? 4.0f : 1.0f;
+}
+
+// Slot weight s of cell k, as the stencil's accumulation type.
+template <bool MP>
+__device__ __forceinline__ typename Prec<MP>::A slot_w(const StencilDev &S, int s, int k) {
+    if (MP) {
+        if (S.wslot_h) return __half2float(S.wslot_h[s * S.n + k]);
+        return __ldg(S.wslot + s * S.n + k);
+    }
+    return __ldg(S.wslot_d + s * S.n + k);
+}
 
 // Phase trace (diagnostics): block 0, thread 0 records (mark, %globaltimer).
 __device__ int g_trace_n;
@@ -123,27 +196,27 @@ struct Own {
 
 // cell(c, x, wE, wN, wNE, wNW, rsum, r0, o) for every cell c of this block's
 // range of a level.  Over the stencil window of the current sub-range, x[k] =
-// load(k, mine, o) and the four slot weights are staged (FP64) in shared
-// memory; for the cells of the sub-range (mine) load also fills o, whose a, b,
-// c are staged too, and commit(k, o) then performs the cell's side effects
-// (global stores) after the loads of the pass are issued.  load must not
-// store.  The links that leave a face (boundary-ring cells) are summed while
-// staging as well: rsum[ring rank - r0] = sum_k w_k (x(c) - x(nb_k)), one
-// thread per ring cell.  All global loads happen while staging, where they are
-// independent, so the compute loop reads shared memory only.  Ends with a
-// block barrier.
-template <class Load, class Commit, class Cell>
-__device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load load, Commit commit, Cell cell) {
+// load(k, mine, o) and the four slot weights are staged (accumulation type A:
+// FP64 plain, FP32 mixed) in shared memory; for the cells of the sub-range
+// (mine) load also fills o, whose a, b, c are staged too, and commit(k, o)
+// then performs the cell's side effects (global stores) after the loads of
+// the pass are issued.  load must not store.  The links that leave a face
+// (boundary-ring cells) are summed while staging as well: rsum[ring rank - r0]
+// = sum_k w_k (x(c) - x(nb_k)), one thread per ring cell.  All global loads
+// happen while staging, where they are independent, so the compute loop reads
+// shared memory only.  Ends with a block barrier.
+template <bool MP, class Load, class Commit, class Cell>
+__device__ __forceinline__ void staged(const StencilDev &S, double *raw, Load load, Commit commit, Cell cell) {
+    using A = typename Prec<MP>::A;
     const int N = S.N, n = S.n, nring = S.nring, bs = blockDim.x, tid = threadIdx.x;
     int c0, c1;
     block_range(n, N, c0, c1);
     const int halo = N + 1;
     const int sub = kStageCap - 2 * halo;
-    double *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap,
-           *b3 = buf + 4 * kStageCap;
+    A *buf = reinterpret_cast<A *>(raw);
+    A *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap, *b3 = buf + 4 * kStageCap;
     float *oa = reinterpret_cast<float *>(buf + 5 * kStageCap), *ob = oa + kStageCap, *oc = ob + kStageCap;
-    double *rs = buf + kStageWords - kRingCap;
-    const double *wd = S.wslot_d;
+    A *rs = reinterpret_cast<A *>(oc + kStageCap);
     stage_mark(1);
     for (int s0 = c0; s0 < c1;) {
         int s1 = min(c1, s0 + sub);
@@ -166,7 +239,7 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
         const float4 *rw4 = reinterpret_cast<const float4 *>(S.ring_w) + 2 * (size_t)r0;
         int4 fo0 = make_int4(-1, -1, -1, -1), fo1 = fo0;
         float4 fw0 = make_float4(0.f, 0.f, 0.f, 0.f), fw1 = fw0;
-        double fvc = 0;
+        A fvc = 0;
         if (tid < nr) {
             fo0 = __ldg(rn4 + 2 * tid);
             fo1 = __ldg(rn4 + 2 * tid + 1);
@@ -184,20 +257,20 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
             const bool two = k2 < w1;
             const bool in1 = k >= s0 && k < s1, in2 = two && k2 >= s0 && k2 < s1;
             Own o1{0.f, 0.f, 0.f, 0.f}, o2{0.f, 0.f, 0.f, 0.f};
-            double e1 = 0, n1 = 0, ne1 = 0, nw1 = 0, v1 = 0;
+            A e1 = 0, n1 = 0, ne1 = 0, nw1 = 0, v1 = 0;
             if (k >= 0 && k < n) {
-                e1 = __ldg(wd + k);
-                n1 = __ldg(wd + n + k);
-                ne1 = __ldg(wd + 2 * n + k);
-                nw1 = __ldg(wd + 3 * n + k);
+                e1 = slot_w<MP>(S, 0, k);
+                n1 = slot_w<MP>(S, 1, k);
+                ne1 = slot_w<MP>(S, 2, k);
+                nw1 = slot_w<MP>(S, 3, k);
                 v1 = load(k, in1, o1);
             }
-            double e2 = 0, n2 = 0, ne2 = 0, nw2 = 0, v2 = 0;
+            A e2 = 0, n2 = 0, ne2 = 0, nw2 = 0, v2 = 0;
             if (two && k2 >= 0 && k2 < n) {
-                e2 = __ldg(wd + k2);
-                n2 = __ldg(wd + n + k2);
-                ne2 = __ldg(wd + 2 * n + k2);
-                nw2 = __ldg(wd + 3 * n + k2);
+                e2 = slot_w<MP>(S, 0, k2);
+                n2 = slot_w<MP>(S, 1, k2);
+                ne2 = slot_w<MP>(S, 2, k2);
+                nw2 = slot_w<MP>(S, 3, k2);
                 v2 = load(k2, in2, o2);
             }
             if (in1) commit(k, o1);
@@ -233,7 +306,7 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
         for (int q = tid; q < nr; q += bs) {
             int4 o0, o1;
             float4 w0v, w1v;
-            double vc;
+            A vc;
             if (q == tid) {
                 o0 = fo0;
                 o1 = fo1;
@@ -252,23 +325,23 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
             }
             const int o[8] = {o0.x, o0.y, o0.z, o0.w, o1.x, o1.y, o1.z, o1.w};
             const float w[8] = {w0v.x, w0v.y, w0v.z, w0v.w, w1v.x, w1v.y, w1v.z, w1v.w};
-            double v[8];
+            A v[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 Own none;
                 v[k] = o[k] >= 0 ? load(o[k], false, none) : vc;
             }
-            double t = 0;
+            A t = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++)
-                if (o[k] >= 0) t += (double)w[k] * (vc - v[k]);
+                if (o[k] >= 0) t += (A)w[k] * (vc - v[k]);
             rs[q] = t;
         }
         __syncthreads();
         stage_mark(2);
         // two independent cells in flight per thread: one cell's dependent
-        // chain (shared loads, FP64 sum, conversions) leaves the issue slots
-        // idle with 16 warps per SM
+        // chain (shared loads, sum, conversions) leaves the issue slots idle
+        // with 16 warps per SM
 #pragma unroll 2
         for (int c = s0 + tid; c < s1; c += bs) {
             Own o;
@@ -283,26 +356,31 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *buf, Load lo
     }
 }
 
-#define STAGED_ARGS                                                                                             \
-    const double *x, const double *wE, const double *wN, const double *wNE, const double *wNW, const double *rsum, \
+#define STAGED_ARGS                                                                                            \
+    const typename Prec<MP>::A *x, const typename Prec<MP>::A *wE, const typename Prec<MP>::A *wN,           \
+        const typename Prec<MP>::A *wNE, const typename Prec<MP>::A *wNW, const typename Prec<MP>::A *rsum, \
         int r0, Own o
 #define APPLY(S, c, xc) apply_k_smem(S, c, xc, x, wE, wN, wNE, wNW, rsum, r0)
 
-// The pre-smoothed iterate from 0 at cell k: w D^-1 b.
+// The pre-smoothed iterate from 0 at cell k: w D^-1 b (as stored).
+template <bool MP>
 __device__ __forceinline__ float presmooth_x(const LevelDev &L, int k, float b) {
+    if (MP) return as_stored<true>(0.8f * __ldg(L.dinv + k) * b);
     return (float)(kOmegaJ * __ldg(L.dinv + k) * b);
 }
 
-// (R r_fine) at coarse cell c.  Interior coarse cells gather their 4x4 fine
-// window in the CSR row order (fine index ascending) with the P weights; the
-// others use the CSR rows.
+// (R r_fine) at coarse cell c (times 1/4 in the mixed V-cycle).  Interior
+// coarse cells gather their 4x4 fine window in the CSR row order (fine index
+// ascending) with the P weights; the others use the CSR rows.
+template <bool MP>
 __device__ __forceinline__ float restrict_value(const LevelDev &F, const LevelDev &C, int c) {
+    using A = typename Prec<MP>::A;
     const int Nc = C.S.N, Nf = F.S.N;
+    const auto *r = lv<MP>(F.r);
     int f, I, J;
     cell_fij(C.S, c, f, I, J);
-    double acc = 0;
+    A acc = 0;
     if (F.structured && I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc) {
-        const float *r = F.r;
         const int base = (f * Nf + 2 * J - 1) * Nf + 2 * I - 1;
         const int nc = C.S.n;
         float wv[16], rv[16];
@@ -312,26 +390,29 @@ __device__ __forceinline__ float restrict_value(const LevelDev &F, const LevelDe
             for (int di = 0; di < 4; di++) {
                 const int i = base + dj * Nf + di;
                 wv[dj * 4 + di] = __ldg(F.rw16 + (dj * 4 + di) * nc + c);
-                rv[dj * 4 + di] = r[i];
+                rv[dj * 4 + di] = ldv(r, i);
             }
 #pragma unroll
-        for (int q = 0; q < 16; q++) acc += (double)(wv[q] * rv[q]);
+        for (int q = 0; q < 16; q++) acc += (A)(wv[q] * rv[q]);
     } else {
         const int k0 = __ldg(F.rstart + c), k1 = __ldg(F.rstart + c + 1);
-        for (int k = k0; k < k1; k++) acc += (double)(__ldg(F.rw + k) * F.r[__ldg(F.ridx + k)]);
+        for (int k = k0; k < k1; k++) acc += (A)(__ldg(F.rw + k) * ldv(r, __ldg(F.ridx + k)));
     }
-    return (float)acc;
+    return (float)acc * restrict_scale<MP>();
 }
+template <bool MP>
 __device__ __forceinline__ void restrict_cell(const LevelDev &F, const LevelDev &C, int c) {
-    C.b[c] = restrict_value(F, C, c);
+    stv(lv<MP>(C.b), c, restrict_value<MP>(F, C, c));
 }
 
-// x_fine + P xo_coarse at fine cell i.  Interior fine cells compute their 2x2
-// coarse taps.
+// x_fine + P xo_coarse (times 4 in the mixed V-cycle) at fine cell i.
+// Interior fine cells compute their 2x2 coarse taps.
+template <bool MP>
 __device__ __forceinline__ float prolong_value(const LevelDev &F, const LevelDev &C, int i) {
     const int Nf = F.S.N, Nc = C.S.N;
+    (void)Nf;
     const float4 w = __ldg(reinterpret_cast<const float4 *>(F.pw) + i);
-    const float *xc = C.xo;
+    const auto *xc = lv<MP>(C.xo);
     int t0, t1, t2, t3;
     int f, fi, fj;
     cell_fij(F.S, i, f, fi, fj);
@@ -348,89 +429,105 @@ __device__ __forceinline__ float prolong_value(const LevelDev &F, const LevelDev
         t2 = t.z;
         t3 = t.w;
     }
-    const float s = w.x * xc[t0] + w.y * xc[t1] + w.z * xc[t2] + w.w * xc[t3];
-    return F.x[i] + (float)(kCorrScale * s);
-}
-__device__ __forceinline__ void prolong_cell(const LevelDev &F, const LevelDev &C, int i) {
-    F.x[i] = prolong_value(F, C, i);
+    const float s = w.x * ldv(xc, t0) + w.y * ldv(xc, t1) + w.z * ldv(xc, t2) + w.w * ldv(xc, t3);
+    if (MP) return ldv(lv<MP>(F.x), i) + 4.0f * s;
+    return ldv(lv<MP>(F.x), i) + (float)(kCorrScale * s);
 }
 
-// Pre-smooth of a level from x = 0 with right-hand side b: x = w D^-1 b,
-// r = b - K x.
-__device__ __forceinline__ void phase_presmooth(const LevelDev &L, const float *b, double *buf) {
-    auto load = [&](int k, bool mine, Own &o) -> double {
-        const float bk = b[k];
+// Pre-smooth of a level from x = 0 with right-hand side bscale * b:
+// x = w D^-1 b, r = b - K x.
+template <bool MP, class TB>
+__device__ __forceinline__ void phase_presmooth(const LevelDev &L, const TB *b, float bscale, double *buf) {
+    using A = typename Prec<MP>::A;
+    auto load = [&](int k, bool mine, Own &o) -> A {
+        const float bk = MP ? ldv(b, k) * bscale : ldv(b, k);
         if (mine) o.a = bk;
-        return (double)presmooth_x(L, k, bk);
+        return (A)presmooth_x<MP>(L, k, bk);
     };
     auto commit = [&](int, const Own &) {};
-    staged(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
+    auto *lx = lv<MP>(L.x);
+    auto *lr = lv<MP>(L.r);
+    staged<MP>(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
         const float bc = o.a;
         const float xc = (float)x[c];  // = presmooth_x(L, c, bc)
-        const double kx = APPLY(L.S, c, (double)xc);
-        L.x[c] = xc;
-        L.r[c] = (float)(bc - kx);
+        const A kx = APPLY(L.S, c, (A)xc);
+        stv(lx, c, xc);
+        stv(lr, c, (float)(bc - kx));
     });
 }
 
 // Prolongation C -> L fused with L's post-smooth: x = x_L + P xo_C is formed on
-// the fly over the staged window (never stored), then xo = x + w D^-1 (b - K x);
-// returns sum dotr . xo when dotr != nullptr.  Same arithmetic as a separate
-// prolongation pass followed by the post-smooth, one grid barrier fewer.
-__device__ __forceinline__ double phase_prolong_postsmooth(const LevelDev &L, const LevelDev &C, const float *b,
-                                                           float *xo, const float *dotr, double *buf) {
-    double s = 0;
-    auto load = [&](int k, bool mine, Own &o) -> double {
+// the fly over the staged window (never stored), then xo = x + w D^-1 (b - K x)
+// with b = bscale * b_in, stored as oscale * xo; returns sum dotr . (oscale xo)
+// in s (and sum dotr . zold in so) when dotr != nullptr.  Same arithmetic as a
+// separate prolongation pass followed by the post-smooth, one grid barrier fewer.
+template <bool MP, class TB, class TO>
+__device__ __forceinline__ void phase_prolong_postsmooth(const LevelDev &L, const LevelDev &C, const TB *b,
+                                                         float bscale, TO *xo, float oscale, const float *dotr,
+                                                         const float *zold, double &s, double &so, double *buf) {
+    using A = typename Prec<MP>::A;
+    auto load = [&](int k, bool mine, Own &o) -> A {
         if (mine) {
-            o.a = b[k];
+            o.a = MP ? ldv(b, k) * bscale : ldv(b, k);
             o.b = __ldg(L.dinv + k);
             o.c = dotr ? dotr[k] : 0.f;
+            if (MP) o.d = zold ? zold[k] : 0.f;
         }
-        return (double)prolong_value(L, C, k);
+        return (A)prolong_value<MP>(L, C, k);
     };
-    auto commit = [&](int, const Own &) {};
-    staged(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
+    double so_ = 0;
+    auto commit = [&](int, const Own &o) {
+        if (MP) so_ += (double)o.c * o.d;
+    };
+    staged<MP>(L.S, buf, load, commit, [&](int c, STAGED_ARGS) {
         const float xc = (float)x[c];
-        const float rc = (float)(o.a - APPLY(L.S, c, (double)xc));
-        const float out = xc + (float)(kOmegaJ * o.b * rc);
-        xo[c] = out;
-        s += (double)o.c * out;
+        const float rc = (float)(o.a - APPLY(L.S, c, (A)xc));
+        float out;
+        if (MP)
+            out = (xc + 0.8f * o.b * rc) * oscale;
+        else
+            out = xc + (float)(kOmegaJ * o.b * rc);
+        s += (double)o.c * stv_get(xo, c, out);
     });
-    return s;
+    so = so_;
 }
 
 // One damped-Jacobi sweep src -> dst with per-link conversions (small levels).
-__device__ __forceinline__ float jacobi_cell(const StencilDev &S, const float *dinv, const float *b, const float *src,
-                                             float *dst, int c) {
-    auto X = [&](int k) -> double { return (double)src[k]; };
-    float xc = src[c];
-    float rc = (float)(b[c] - apply_k(S, c, (double)xc, X));
+template <bool MP>
+__device__ __forceinline__ float jacobi_cell(const StencilDev &S, const float *dinv, const typename Prec<MP>::V *b,
+                                             const typename Prec<MP>::V *src, typename Prec<MP>::V *dst, int c) {
+    auto X = [&](int k) -> double { return (double)ldv(src, k); };
+    float xc = ldv(src, c);
+    float rc = (float)(ldv(b, c) - apply_k(S, c, (double)xc, X));
     float out = xc + (float)(kOmegaJ * __ldg(dinv + c) * rc);
-    dst[c] = out;
+    stv(dst, c, out);
     return out;
 }
 
 // ---- the coarse levels inside one block (setup of the dense map, fallback) --
+// Always FP32 vectors in shared memory with the plain arithmetic: the V-cycle
+// of these levels maps b_l0 to xo_l0 the same way in both precisions (the
+// mixed transfer factors 1/4 and 4 cancel within it).
 
 struct SmemLevel {
     float *x, *xo, *b, *r;
 };
 
-__device__ void carve_smem(const SolveParams &P, int l0, float *smem, SmemLevel *lv) {
+__device__ void carve_smem(const SolveParams &P, int l0, float *smem, SmemLevel *lv_) {
     float *q = smem;
     for (int l = l0; l < P.nlev; l++) {
         int n = P.L[l].S.n;
-        lv[l].x = q;
-        lv[l].xo = q + n;
-        lv[l].b = q + 2 * n;
-        lv[l].r = q + 3 * n;
+        lv_[l].x = q;
+        lv_[l].xo = q + n;
+        lv_[l].b = q + 2 * n;
+        lv_[l].r = q + 3 * n;
         q += 4 * n;
     }
 }
 
 // Coarsest level: `sweeps` Jacobi sweeps from 0; result in V.xo.  When every
 // cell has its own thread, the cell's links, 1/diag and b stay in registers.
-__device__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps) {
+__device__ __noinline__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps) {
     const int n = L.S.n;
     BLOCK_LOOP(c, n) V.x[c] = 0.f;
     __syncthreads();
@@ -461,7 +558,7 @@ __device__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps)
         }
     } else {
         for (int s = 0; s < sweeps; s++) {
-            BLOCK_LOOP(c, n) jacobi_cell(L.S, L.dinv, V.b, src, dst, c);
+            BLOCK_LOOP(c, n) jacobi_cell<false>(L.S, L.dinv, V.b, src, dst, c);
             __syncthreads();
             float *t = src;
             src = dst;
@@ -475,115 +572,128 @@ __device__ void coarsest_smem(const LevelDev &L, const SmemLevel &V, int sweeps)
 }
 
 // Levels l0..nlev-1 of the V-cycle inside this block, on vectors in shared
-// memory.  b of level l0 is lv[l0].b on entry; xo of level l0 is written to
-// `out` (global memory).
-__device__ void vcycle_block_smem(const SolveParams &P, int l0, SmemLevel *lv, float *out) {
+// memory.  b of level l0 is lv[l0].b on entry; xo of level l0 is left in
+// lv[l0].xo.  Not inlined (with coarsest_smem): a fallback and set-up path
+// whose locals would otherwise crowd the solve kernel's registers.
+__device__ __noinline__ void vcycle_block_smem(const SolveParams &P, int l0, SmemLevel *lv_) {
     const int last = P.nlev - 1;
     for (int l = l0; l < last; l++) {
         LevelDev L = P.L[l];
-        L.x = lv[l].x;
-        L.r = lv[l].r;
-        const float *b = lv[l].b;
+        L.x = lv_[l].x;
+        L.r = lv_[l].r;
+        const float *b = lv_[l].b;
+        float *lx = lv_[l].x, *lr = lv_[l].r;
         BLOCK_LOOP(c, L.S.n) {
             auto X = [&](int k) -> double { return (double)(float)(kOmegaJ * __ldg(L.dinv + k) * b[k]); };
             float bc = b[c];
             float xc = (float)(kOmegaJ * __ldg(L.dinv + c) * bc);
             double kx = apply_k(L.S, c, (double)xc, X);
-            L.x[c] = xc;
-            L.r[c] = (float)(bc - kx);
+            lx[c] = xc;
+            lr[c] = (float)(bc - kx);
         }
         __syncthreads();
         LevelDev C = P.L[l + 1];
-        C.b = lv[l + 1].b;
-        BLOCK_LOOP(c, C.S.n) restrict_cell(L, C, c);
+        C.b = lv_[l + 1].b;
+        BLOCK_LOOP(c, C.S.n) restrict_cell<false>(L, C, c);
         __syncthreads();
     }
-    coarsest_smem(P.L[last], lv[last], P.coarse_sweeps);
+    coarsest_smem(P.L[last], lv_[last], P.coarse_sweeps);
     for (int l = last - 1; l >= l0; l--) {
         LevelDev L = P.L[l];
-        L.x = lv[l].x;
+        L.x = lv_[l].x;
         LevelDev C = P.L[l + 1];
-        C.xo = lv[l + 1].xo;
-        BLOCK_LOOP(i, L.S.n) prolong_cell(L, C, i);
+        C.xo = lv_[l + 1].xo;
+        BLOCK_LOOP(i, L.S.n) lv_[l].x[i] = prolong_value<false>(L, C, i);
         __syncthreads();
-        BLOCK_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, lv[l].b, lv[l].x, lv[l].xo, c);
+        BLOCK_LOOP(c, L.S.n) jacobi_cell<false>(L.S, L.dinv, lv_[l].b, lv_[l].x, lv_[l].xo, c);
         __syncthreads();
     }
-    BLOCK_LOOP(c, P.L[l0].S.n) out[c] = lv[l0].xo[c];
-    __syncthreads();
 }
 
 // ---- the V-cycle after level 0's pre-smooth --------------------------------
 
 // The rest of z = V(r) once level 0's pre-smooth (x, r of level 0) is complete
-// and visible.  Ends with rz = r . z published; returns false on abort.
-__device__ bool vcycle_rest(const SolveParams &P, const float *r, double *s_red, double *buf, float *smem) {
+// and visible; the V-cycle ran on s0 * r (s0 = 1 in the plain solve).  Ends
+// with rz = r . z (and, mixed, r . z_prev) published; returns false on abort.
+template <bool MP>
+__device__ bool vcycle_rest(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
+                            double *s_red, double *buf, float *smem) {
     const int G = P.nlev_grid;
     // down
     for (int l = 0; l < G; l++) {
         const LevelDev &L = P.L[l];
         if (l > 0) {
-            phase_presmooth(L, L.b, buf);
+            phase_presmooth<MP>(L, lv<MP>(L.b), 1.0f, buf);
             trace_mark(P, 100 + l);
             SYNC_OR(return false);
         }
-        GRID_LOOP(c, P.L[l + 1].S.n) restrict_cell(L, P.L[l + 1], c);
+        GRID_LOOP(c, P.L[l + 1].S.n) restrict_cell<MP>(L, P.L[l + 1], c);
         trace_mark(P, 300 + l);
         SYNC_OR(return false);
     }
     // below the grid levels: the dense map, or block 0
     if (P.dense) {
         const LevelDev &C = P.L[G];
+        const auto *cb = lv<MP>(C.b);
+        auto *cx = lv<MP>(C.xo);
         const int nd = P.nd, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
         for (int row = gw; row < nd; row += nw) {
             const double *d = P.dense + (size_t)row * nd;
             double acc = 0;
-            for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)C.b[j];
+            for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)ldv(cb, j);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) C.xo[row] = (float)acc;
+            if (lane == 0) stv(cx, row, (float)acc);
         }
         trace_mark(P, 500);
         SYNC_OR(return false);
     } else if (!P.coarse_on_grid) {
         if (blockIdx.x == 0) {
-            SmemLevel lv[kMaxLev];
-            carve_smem(P, G, smem, lv);
-            BLOCK_LOOP(c, P.L[G].S.n) lv[G].b[c] = P.L[G].b[c];
+            SmemLevel lvs[kMaxLev];
+            carve_smem(P, G, smem, lvs);
+            const auto *gb = lv<MP>(P.L[G].b);
+            BLOCK_LOOP(c, P.L[G].S.n) lvs[G].b[c] = ldv(gb, c);
             __syncthreads();
-            vcycle_block_smem(P, G, lv, P.L[G].xo);
+            vcycle_block_smem(P, G, lvs);
+            auto *gx = lv<MP>(P.L[G].xo);
+            BLOCK_LOOP(c, P.L[G].S.n) stv(gx, c, lvs[G].xo[c]);
         }
         trace_mark(P, 500);
         SYNC_OR(return false);
     } else {
         // the coarsest level is large (nlev_grid == nlev - 1): sweep it grid-wide
         const LevelDev &L = P.L[P.nlev - 1];
-        GRID_LOOP(c, L.S.n) L.x[c] = 0.f;
+        auto *lx = lv<MP>(L.x), *lxo = lv<MP>(L.xo);
+        const auto *lb = lv<MP>(L.b);
+        GRID_LOOP(c, L.S.n) stv(lx, c, 0.f);
         SYNC_OR(return false);
-        float *src = L.x, *dst = L.xo;
+        auto *src = lx, *dst = lxo;
         for (int s = 0; s < P.coarse_sweeps; s++) {
-            GRID_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, L.b, src, dst, c);
+            GRID_LOOP(c, L.S.n) jacobi_cell<MP>(L.S, L.dinv, lb, src, dst, c);
             SYNC_OR(return false);
-            float *t = src;
+            auto *t = src;
             src = dst;
             dst = t;
         }
-        if (src != L.xo) {
-            GRID_LOOP(c, L.S.n) L.xo[c] = src[c];
+        if (src != lxo) {
+            GRID_LOOP(c, L.S.n) lxo[c] = src[c];
             SYNC_OR(return false);
         }
     }
     // up: prolongation fused with each grid level's post-smooth
     for (int l = G - 1; l >= 0; l--) {
         const LevelDev &L = P.L[l];
+        double s = 0, so = 0;
         if (l > 0) {
-            phase_prolong_postsmooth(L, P.L[l + 1], L.b, L.xo, nullptr, buf);
+            phase_prolong_postsmooth<MP>(L, P.L[l + 1], lv<MP>(L.b), 1.0f, lv<MP>(L.xo), 1.0f, nullptr, nullptr, s, so,
+                                         buf);
             trace_mark(P, 900 + l);
             SYNC_OR(return false);
         } else {
-            double s = phase_prolong_postsmooth(L, P.L[1], r, P.z, r, buf);
+            phase_prolong_postsmooth<MP>(L, P.L[1], r, s0, z, 1.0f / s0, r, zold, s, so, buf);
             put_partial(P, RED_RZ, s, s_red);
+            if (MP) put_partial(P, RED_RZO, so, s_red);
             trace_mark(P, 900);
             SYNC_OR(return false);
         }
@@ -591,59 +701,83 @@ __device__ bool vcycle_rest(const SolveParams &P, const float *r, double *s_red,
     return true;
 }
 
-// z = V(r) for a single-level hierarchy (level 0 is the coarsest grid).
-__device__ bool single_level(const SolveParams &P, const float *r, double *s_red, float *smem) {
+// z = V(r) for a single-level hierarchy (level 0 is the coarsest grid); the
+// sweeps run on s0 * r (s0 = 1 in the plain solve).
+template <bool MP>
+__device__ bool single_level(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
+                             double *s_red, float *smem) {
     const LevelDev &L = P.L[0];
+    auto *lx = lv<MP>(L.x), *lxo = lv<MP>(L.xo);
+    auto *lb = lv<MP>(L.b);
     if (!P.coarse_on_grid) {
         if (blockIdx.x == 0) {
-            SmemLevel lv[kMaxLev];
-            carve_smem(P, 0, smem, lv);
-            BLOCK_LOOP(c, L.S.n) lv[0].b[c] = r[c];
+            SmemLevel lvs[kMaxLev];
+            carve_smem(P, 0, smem, lvs);
+            BLOCK_LOOP(c, L.S.n) lvs[0].b[c] = r[c];
             __syncthreads();
-            coarsest_smem(L, lv[0], P.coarse_sweeps);
-            BLOCK_LOOP(c, L.S.n) L.xo[c] = lv[0].xo[c];
+            coarsest_smem(L, lvs[0], P.coarse_sweeps);
+            BLOCK_LOOP(c, L.S.n) stv(lxo, c, MP ? lvs[0].xo[c] * s0 : lvs[0].xo[c]);
         }
     } else {
-        GRID_LOOP(c, L.S.n) L.x[c] = 0.f;
+        GRID_LOOP(c, L.S.n) {
+            stv(lx, c, 0.f);
+            stv(lb, c, MP ? r[c] * s0 : r[c]);
+        }
         SYNC_OR(return false);
-        float *src = L.x, *dst = L.xo;
+        auto *src = lx, *dst = lxo;
         for (int s = 0; s < P.coarse_sweeps; s++) {
-            GRID_LOOP(c, L.S.n) jacobi_cell(L.S, L.dinv, r, src, dst, c);
+            GRID_LOOP(c, L.S.n) jacobi_cell<MP>(L.S, L.dinv, lb, src, dst, c);
             SYNC_OR(return false);
-            float *t = src;
+            auto *t = src;
             src = dst;
             dst = t;
         }
-        if (src != L.xo) {
-            GRID_LOOP(c, L.S.n) L.xo[c] = src[c];
+        if (src != lxo) {
+            GRID_LOOP(c, L.S.n) lxo[c] = src[c];
         }
     }
     SYNC_OR(return false);
-    double s = 0;
+    double s = 0, so = 0;
+    const float inv = 1.0f / s0;
     GRID_LOOP(c, L.S.n) {
-        float z = L.xo[c];
-        P.z[c] = z;
-        s += (double)r[c] * z;
+        if (zold) so += (double)r[c] * zold[c];
+        float zc = MP ? ldv(lxo, c) * inv : ldv(lxo, c);
+        z[c] = zc;
+        s += (double)r[c] * zc;
     }
     put_partial(P, RED_RZ, s, s_red);
+    if (MP) put_partial(P, RED_RZO, so, s_red);
     return grid_sync(P.bar);
 }
 
+// Power of two that brings a residual of squared norm rr over n cells to an
+// RMS near 1/16 (the mixed V-cycle's input scale; 1 in the plain solve).
+template <bool MP>
+__device__ __forceinline__ float vscale(double rr, int n) {
+    if (!MP || !(rr > 0) || !isfinite(rr)) return 1.0f;
+    const int e = ilogb(sqrt(rr / n));
+    return ldexpf(1.0f, max(-100, min(100, -4 - e)));
+}
+
+template <bool MP>
 __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     __shared__ Red sh;
     extern __shared__ __align__(16) unsigned char dyn[];
     double *buf = reinterpret_cast<double *>(dyn);               // staged window
     float *smem = reinterpret_cast<float *>(dyn + kStageBytes);  // block-0 levels
     double *s_red = sh.v;
+    using A = typename Prec<MP>::A;
     const LevelDev &L0 = P.L[0];
     const StencilDev &S0 = L0.S;
     const int n = S0.n;
     const bool mg = P.nlev >= 2;
     const bool single = P.nlev == 1;
     float *r = P.r, *rn = P.r2, *p = P.p, *pn = P.p2;
+    float *z = P.z, *zo = MP ? P.z2 : nullptr;  // mixed: z / z2 ping-pong (the previous z for the flexible beta)
     double bb, rr, rz = 0, tol2, beta = 0, m2;
-    int it = 0;
+    int it = 0, flags = 0;
     bool first = true, ok = true;
+    float s0 = 1.0f;
 
     // zero-mean projection of omega (FP64 sum), upstream src/fluid.c:264-275
     if (P.remove_mean) {
@@ -678,17 +812,17 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     {
         double sb = 0, sr = 0;
         const float *psi = P.psi;
-        auto load = [&](int k, bool mine, Own &o) -> double {
+        auto load = [&](int k, bool mine, Own &o) -> A {
             if (mine) {
                 o.a = P.omega[k];
                 o.b = __ldg(P.area + k);
             }
-            return (double)psi[k];
+            return (A)psi[k];
         };
         auto commit = [&](int, const Own &) {};
-        staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
+        staged<MP>(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
             double b = -(double)o.b * ((double)o.a - m2);
-            double ri = b - APPLY(S0, c, x[c]);
+            double ri = b - (double)APPLY(S0, c, x[c]);
             r[c] = (float)ri;
             sb += b * b;
             sr += ri * ri;
@@ -699,6 +833,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     SYNC_OR(goto aborted);
     bb = get_total(P, RED_BB, s_red);
     rr = get_total(P, RED_RR, s_red);
+    if (!isfinite(bb) || !isfinite(rr)) flags |= kSolveNonFinite;
     if (bb == 0.0) {
         GRID_LOOP(c, n) P.psi[c] = 0.f;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -706,6 +841,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             P.res->relres = 0;
             P.res->status = 0;
             P.res->r_final = 0;
+            P.res->flags = flags;
         }
         return;
     }
@@ -714,43 +850,46 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     // z = M^-1 r, rz
     if (rr > tol2) {
         if (mg) {
-            phase_presmooth(L0, r, buf);
+            s0 = vscale<MP>(rr, n);
+            phase_presmooth<MP>(L0, r, s0, buf);
             SYNC_OR(goto aborted);
-            ok = vcycle_rest(P, r, s_red, buf, smem);
+            ok = vcycle_rest<MP>(P, r, s0, z, nullptr, s_red, buf, smem);
         } else if (single) {
-            ok = single_level(P, r, s_red, smem);
+            s0 = vscale<MP>(rr, n);
+            ok = single_level<MP>(P, r, s0, z, nullptr, s_red, smem);
         } else {
             double s = 0;
             GRID_LOOP(c, n) {
-                float z = __ldg(L0.dinv + c) * r[c];
-                P.z[c] = z;
-                s += (double)r[c] * z;
+                float zc = __ldg(L0.dinv + c) * r[c];
+                z[c] = zc;
+                s += (double)r[c] * zc;
             }
             put_partial(P, RED_RZ, s, s_red);
             ok = grid_sync(P.bar);
         }
         if (!ok) goto aborted;
         rz = get_total(P, RED_RZ, s_red);
+        if (!isfinite(rz)) flags |= kSolveNonFinite;
     }
 
     while (rr > tol2 && it < P.maxit) {
         // p = z (first) or z + beta p;  Ap = K p;  pAp
         {
-            const float *z = P.z;
+            const float *zz = z;
             const float *po = p;
             const bool fst = first;
             const double be = beta;
-            auto pnew = [&](int k) -> float { return fst ? z[k] : (float)(z[k] + be * po[k]); };
-            auto load = [&](int k, bool, Own &) -> double { return (double)pnew(k); };
+            auto pnew = [&](int k) -> float { return fst ? zz[k] : (float)(zz[k] + be * po[k]); };
+            auto load = [&](int k, bool, Own &) -> A { return (A)pnew(k); };
             auto commit = [&](int, const Own &) {};
             double s = 0;
             float *pw = pn, *ap = P.Ap;
-            staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
+            staged<MP>(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
                 const float pc = (float)x[c];
-                const double a = APPLY(S0, c, (double)pc);
+                const A a = APPLY(S0, c, (A)pc);
                 pw[c] = pc;
                 ap[c] = (float)a;
-                s += a * pc;
+                s += (double)a * pc;
             });
             put_partial(P, RED_PAP, s, s_red);
             float *t = p;
@@ -763,7 +902,11 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         trace_mark(P, 11);
         {
             double pAp = get_total(P, RED_PAP, s_red);
-            if (pAp <= 0) break;
+            if (!isfinite(pAp)) flags |= kSolveNonFinite;
+            if (pAp <= 0) {
+                flags |= kSolveBreakdown;
+                break;
+            }
             const double alpha = rz / pAp;
             const float *Ap = P.Ap;
             const float *ro = r;
@@ -771,29 +914,34 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
             double s = 0, sz = 0;
             float *rw_ = rn;
             if (mg) {
+                // the previous r's scale (the new r is not reduced yet)
+                s0 = vscale<MP>(rr, n);
+                const float sc = s0;
                 // psi += alpha p; r' = r - alpha Ap; level-0 pre-smooth of r'
                 auto rnew = [&](int k) -> float { return (float)(ro[k] - alpha * Ap[k]); };
                 // mine: r, Ap of the cell staged; p and psi kept for commit,
                 // which does psi += alpha p (nothing else reads psi)
-                auto load = [&](int k, bool mine, Own &o) -> double {
+                auto load = [&](int k, bool mine, Own &o) -> A {
                     if (mine) {
                         o.a = ro[k];
                         o.b = Ap[k];
                         o.c = pp[k];
                         o.d = P.psi[k];
                     }
-                    return (double)presmooth_x(L0, k, rnew(k));
+                    return (A)presmooth_x<MP>(L0, k, MP ? rnew(k) * sc : rnew(k));
                 };
                 auto commit = [&](int k, const Own &o) { P.psi[k] = o.d + (float)(alpha * o.c); };
-                staged(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
+                auto *l0x = lv<MP>(L0.x);
+                auto *l0r = lv<MP>(L0.r);
+                staged<MP>(S0, buf, load, commit, [&](int c, STAGED_ARGS) {
                     const double ri = o.a - alpha * o.b;
                     const float rc = (float)ri;
                     rw_[c] = rc;
                     s += ri * ri;
-                    const float xc = (float)x[c];  // = presmooth_x(L0, c, rc)
-                    const double kx = APPLY(S0, c, (double)xc);
-                    L0.x[c] = xc;
-                    L0.r[c] = (float)(rc - kx);
+                    const float xc = (float)x[c];  // = presmooth_x(L0, c, rc * sc)
+                    const A kx = APPLY(S0, c, (A)xc);
+                    stv(l0x, c, xc);
+                    stv(l0r, c, (float)((MP ? rc * sc : rc) - kx));
                 });
             } else {
                 GRID_LOOP(c, n) {
@@ -803,9 +951,9 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
                     rw_[c] = rc;
                     s += ri * ri;
                     if (!single) {
-                        float z = __ldg(L0.dinv + c) * rc;
-                        P.z[c] = z;
-                        sz += (double)rc * z;
+                        float zc = __ldg(L0.dinv + c) * rc;
+                        z[c] = zc;
+                        sz += (double)rc * zc;
                     }
                 }
                 if (!single) put_partial(P, RED_RZ, sz, s_red);
@@ -820,15 +968,27 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         SYNC_OR(goto aborted);
         trace_mark(P, 13);
         rr = get_total(P, RED_RR, s_red);
+        if (!isfinite(rr)) flags |= kSolveNonFinite;
         if (rr <= tol2) break;
+        if (MP && (mg || single)) {  // the new z goes to the other buffer; zo keeps the previous one
+            float *t = z;
+            z = zo;
+            zo = t;
+        }
         if (mg)
-            ok = vcycle_rest(P, r, s_red, buf, smem);
-        else if (single)
-            ok = single_level(P, r, s_red, smem);
+            ok = vcycle_rest<MP>(P, r, s0, z, MP ? zo : nullptr, s_red, buf, smem);
+        else if (single) {
+            s0 = vscale<MP>(rr, n);
+            ok = single_level<MP>(P, r, s0, z, MP ? zo : nullptr, s_red, smem);
+        }
         if (!ok) goto aborted;
         {
             double rznew = get_total(P, RED_RZ, s_red);
-            beta = rznew / rz;
+            if (!isfinite(rznew)) flags |= kSolveNonFinite;
+            if (MP && (mg || single))
+                beta = (rznew - get_total(P, RED_RZO, s_red)) / rz;  // Polak-Ribiere
+            else
+                beta = rznew / rz;
             rz = rznew;
         }
     }
@@ -844,15 +1004,18 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     {
         float m = (float)(get_total(P, RED_MEAN, s_red) / P.total_area);
         GRID_LOOP(c, n) P.psi[c] -= m;
-        // leave the final residual / direction in the caller's r / p buffers
+        // leave the final residual / direction / preconditioned residual in the caller's buffers
         if (r != P.r) GRID_LOOP(c, n) P.r[c] = r[c];
         if (p != P.p) GRID_LOOP(c, n) P.p[c] = p[c];
+        if (z != P.z) GRID_LOOP(c, n) P.z[c] = z[c];
     }
+    if (it >= P.maxit && rr > tol2) flags |= kSolveMaxit;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.res->iters = it;
         P.res->relres = sqrt(rr / bb);
         P.res->status = 0;
         P.res->r_final = 0;
+        P.res->flags = flags;
     }
     return;
 
@@ -861,6 +1024,7 @@ aborted:
         P.res->iters = it;
         P.res->relres = -1.0;
         P.res->status = 1;
+        P.res->flags = flags | kSolveTimeout;
     }
 }
 
@@ -868,7 +1032,7 @@ aborted:
 
 // Column j of the dense map of levels l0..nlev-1: the block's V-cycle applied
 // to the unit vector e_j, stored row-major D[row][j] in FP64.
-__global__ void __launch_bounds__(kPB, 1) k_dense_columns(SolveParams P, int l0, float *colbuf, double *D) {
+__global__ void __launch_bounds__(kPB, 1) k_dense_columns(SolveParams P, int l0, double *D) {
     extern __shared__ __align__(16) unsigned char dyn[];
     float *smem = reinterpret_cast<float *>(dyn);
     const int nd = P.L[l0].S.n;
@@ -877,9 +1041,8 @@ __global__ void __launch_bounds__(kPB, 1) k_dense_columns(SolveParams P, int l0,
         carve_smem(P, l0, smem, lv);
         BLOCK_LOOP(c, nd) lv[l0].b[c] = c == j ? 1.0f : 0.0f;
         __syncthreads();
-        float *col = colbuf + (size_t)blockIdx.x * nd;
-        vcycle_block_smem(P, l0, lv, col);
-        BLOCK_LOOP(c, nd) D[(size_t)c * nd + j] = col[c];
+        vcycle_block_smem(P, l0, lv);
+        BLOCK_LOOP(c, nd) D[(size_t)c * nd + j] = lv[l0].xo[c];
         __syncthreads();
     }
 }
@@ -958,30 +1121,34 @@ int pcg_max_blocks() { return 2 * device_sm_count(); }
 // either side) leaves at least one block of threads' worth of cells per pass.
 int pcg_max_grid_n() { return (kStageCap - kPB) / 2 - 1; }
 
+static const void *pcg_kernel(bool mixed) { return mixed ? (const void *)k_pcg<true> : (const void *)k_pcg<false>; }
+
 static void pcg_attributes() {
     static bool attr = false;
     if (!attr) {
         int dev = 0, optin = 0;
         GGB_CHECK(cudaGetDevice(&dev));
         GGB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        cudaFuncAttributes fa;
-        GGB_CHECK(cudaFuncGetAttributes(&fa, k_pcg));
-        GGB_CHECK(cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       optin - (int)fa.sharedSizeBytes));
+        for (int m = 0; m < 2; m++) {
+            cudaFuncAttributes fa;
+            GGB_CHECK(cudaFuncGetAttributes(&fa, pcg_kernel(m)));
+            GGB_CHECK(cudaFuncSetAttribute(pcg_kernel(m), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           optin - (int)fa.sharedSizeBytes));
+        }
         GGB_CHECK(cudaFuncSetAttribute(k_dense_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
 }
 
-static int pcg_grid_for(size_t smem) {
+static int pcg_grid_for(size_t smem, bool mixed) {
     pcg_attributes();
     int per = 0;
-    GGB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg, kPB, smem));
+    GGB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pcg_kernel(mixed), kPB, smem));
     if (per < 1) fail_msg("the solve kernel cannot be resident on this device (%zu B shared memory)", smem);
     return device_sm_count() * std::min(per, 2);
 }
 
-int pcg_grid_size() { return pcg_grid_for(kStageBytes); }
+int pcg_grid_size() { return pcg_grid_for(kStageBytes, false); }
 
 // One solve launch; max_blocks > 0 caps its grid (batched planets: small
 // grids take a share of the SMs so that several solves run at once).
@@ -989,10 +1156,10 @@ void pcg_launch(const SolveParams &prm, cudaStream_t s, int max_blocks) {
     SolveParams p = prm;
     size_t smem = pcg_smem_bytes(p);
     void *args[] = {&p};
-    int grid = pcg_grid_for(smem);
+    int grid = pcg_grid_for(smem, p.mixed != 0);
     if (max_blocks > 0) grid = std::max(1, std::min(grid, max_blocks));
     GGB_CHECK(cudaMemsetAsync(&p.bar->count, 0, sizeof(unsigned int), s));
-    GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(grid), dim3(kPB), args, smem, s));
+    GGB_CHECK(cudaLaunchCooperativeKernel(pcg_kernel(p.mixed != 0), dim3(grid), dim3(kPB), args, smem, s));
     GGB_LAUNCHED();
 }
 
@@ -1026,18 +1193,21 @@ double *pcg_dense_map(const SolveParams &prm, int l0) {
     pcg_attributes();
     int grid = std::min(nd, 4 * device_sm_count());
     double *D = (double *)dev_alloc(sizeof(double) * nd * nd);
-    float *colbuf = (float *)dev_alloc(sizeof(float) * (size_t)grid * nd);
-    k_dense_columns<<<grid, kPB, smem, stream()>>>(p, l0, colbuf, D);
+    k_dense_columns<<<grid, kPB, smem, stream()>>>(p, l0, D);
     GGB_LAUNCHED();
     GGB_CHECK(cudaStreamSynchronize(stream()));
-    dev_free(colbuf);
     return D;
 }
 
 // ---- micro-benchmark of the grid barrier (additive entry point) ----------
-__global__ void __launch_bounds__(kPB, 1) k_barrier_bench(GridBarrier *bar, int rounds, int *ok) {
+// `rounds` barriers with a wait limit of limit_ns each; block `withhold`
+// (-1: none) returns without arriving, so that the others' wait runs out:
+// they raise the barrier's error flag, clear *ok and return.
+__global__ void __launch_bounds__(kPB, 1) k_barrier_bench(GridBarrier *bar, int rounds, int *ok, int withhold,
+                                                        unsigned long long limit_ns) {
+    if ((int)blockIdx.x == withhold) return;
     for (int k = 0; k < rounds; k++)
-        if (!grid_sync(bar)) {
+        if (!grid_sync_limit(bar, limit_ns)) {
             if (threadIdx.x == 0) atomicExch(ok, 0);
             return;
         }
@@ -1045,9 +1215,11 @@ __global__ void __launch_bounds__(kPB, 1) k_barrier_bench(GridBarrier *bar, int 
 
 }  // namespace ggb
 
-// Mean time of one grid-wide barrier of the solve kernel's launch shape, in
-// microseconds (`rounds` barriers in one cooperative launch); -1 on timeout.
-GGB_EXPORT double ggb_barrier_bench(int rounds) {
+// One cooperative launch of `rounds` grid-wide barriers of the solve kernel's
+// launch shape, each wait limited to limit_ms; block `withhold` (-1: none)
+// never arrives.  Returns the launch's duration in ms (*ok = 1 when every
+// barrier completed, 0 when the waits ran out and the kernel returned).
+static double barrier_run(int rounds, int withhold, double limit_ms, int *ok_out) {
     using namespace ggb;
     GridBarrier *bar = (GridBarrier *)dev_alloc(sizeof(GridBarrier));
     int *ok = (int *)dev_alloc(sizeof(int));
@@ -1056,10 +1228,11 @@ GGB_EXPORT double ggb_barrier_bench(int rounds) {
     int per = 0;
     GGB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_barrier_bench, kPB, 0));
     int grid = device_sm_count() * std::min(per, 2);
+    unsigned long long limit_ns = (unsigned long long)(limit_ms * 1e6);
     cudaEvent_t e0, e1;
     GGB_CHECK(cudaEventCreate(&e0));
     GGB_CHECK(cudaEventCreate(&e1));
-    void *args[] = {&bar, &rounds, &ok};
+    void *args[] = {&bar, &rounds, &ok, &withhold, &limit_ns};
     GGB_CHECK(cudaEventRecord(e0, stream()));
     GGB_CHECK(cudaLaunchCooperativeKernel((const void *)k_barrier_bench, dim3(grid), dim3(kPB), args, 0, stream()));
     GGB_LAUNCHED();
@@ -1073,7 +1246,27 @@ GGB_EXPORT double ggb_barrier_bench(int rounds) {
     cudaEventDestroy(e1);
     dev_free(bar);
     dev_free(ok);
-    return hok ? 1000.0 * ms / rounds : -1.0;
+    *ok_out = hok;
+    return ms;
+}
+
+// Mean time of one grid-wide barrier of the solve kernel's launch shape, in
+// microseconds (`rounds` barriers in one cooperative launch); -1 on timeout.
+GGB_EXPORT double ggb_barrier_bench(int rounds) {
+    int ok = 0;
+    double ms = barrier_run(rounds, -1, 2000.0, &ok);
+    return ok ? 1000.0 * ms / rounds : -1.0;
+}
+
+// Failure detection without a fault: one block of a cooperative launch never
+// arrives at the grid barrier, the others wait limit_ms, raise the barrier's
+// error flag and return.  Returns 1 when the waits ran out (0 if the barrier
+// completed after all); *elapsed_ms gets the launch's duration.
+GGB_EXPORT int ggb_barrier_timeout_probe(double limit_ms, double *elapsed_ms) {
+    int ok = 1;
+    double ms = barrier_run(1, 0, limit_ms, &ok);
+    if (elapsed_ms) *elapsed_ms = ms;
+    return ok ? 0 : 1;
 }
 
 // Diagnostics: the next solves record up to `cap` (mark, time in ns) pairs from

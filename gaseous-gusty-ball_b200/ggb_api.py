@@ -161,6 +161,8 @@ class Api:
             ("drv_run", C.c_long, [P(T["CubeSphere"]), P(T["Fluid"]), P(T["Particles"]), P(T["Render"]),
                                    C.c_int, C.c_double, C.c_double, C.c_double, P(C.c_double), P(C.c_int),
                                    P(C.c_double)]),
+            ("ggb_fluid_set_precision", C.c_int, [P(T["Fluid"]), C.c_int]),
+            ("ggb_solve_flags", C.c_int, [P(T["Fluid"])]),
             ("drv_max_threads", C.c_int, []),
             ("drv_set_threads", None, [C.c_int]),
         ]:
@@ -217,13 +219,20 @@ class Grid:
 class FluidSim:
     """Fluid + optional particles / render for one grid."""
 
-    def __init__(self, api, grid, forcing=0.0, rotation=0.0, bfecc=1, cg_tol=1e-4, cg_maxit=500, multigrid=1):
+    def __init__(self, api, grid, forcing=0.0, rotation=0.0, bfecc=1, cg_tol=1e-4, cg_maxit=500, multigrid=1,
+                 mixed=False):
         self.api, self.grid = api, grid
         T = api.T
         self.prm = T["FluidParams"](forcing, rotation, bfecc, cg_tol, cg_maxit, multigrid)
         self.F = T["Fluid"]()
         if api.lib.fluid_init(C.byref(self.F), C.byref(grid.cs), C.byref(self.prm)) != 0:
             raise RuntimeError("fluid_init failed")
+        if mixed:
+            # the mixed-precision solve exists only in the CUDA library
+            if not api.has("ggb_fluid_set_precision"):
+                raise RuntimeError(f"{api.path} has no mixed-precision solve")
+            if api.lib.ggb_fluid_set_precision(C.byref(self.F), 1) != 0:
+                raise RuntimeError("ggb_fluid_set_precision failed")
 
     def field(self, name, comps=1):
         n = self.grid.n

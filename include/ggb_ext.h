@@ -40,6 +40,35 @@ int ggb_stage_times(double *ms, long *count, int n);
 /* Mean cost of one grid-wide barrier of the solve kernel's launch shape (us),
  * measured over `rounds` barriers; -1 if a barrier timed out. */
 double ggb_barrier_bench(int rounds);
+/* Failure detection without a GPU fault: one cooperative launch in which one
+ * block never arrives at the grid barrier; the other blocks give up after
+ * limit_ms, raise the barrier's error flag and return.  Returns 1 when the
+ * waits ran out as they should (0 if the barrier completed), with the
+ * launch's duration in *elapsed_ms.  The device stays usable afterwards. */
+int ggb_barrier_timeout_probe(double limit_ms, double *elapsed_ms);
+/* Status bits of the last Poisson solve of F (fluid_solve_psi, fluid_step,
+ * fluid_set_state, a batched step): GGB_SOLVE_* below, 0 when the solve
+ * converged normally.  The upstream API reports none of these: upstream
+ * src/fluid.c:329-330 ends CG silently on p.Ap <= 0 and a NaN ends it with
+ * relres NaN; the solve here behaves the same and records why. */
+#define GGB_SOLVE_TIMEOUT 1   /* a grid barrier timed out (the process exits, as upstream on OOM) */
+#define GGB_SOLVE_NONFINITE 2 /* NaN or Inf in b.b, r.r, r.z or p.Ap */
+#define GGB_SOLVE_BREAKDOWN 4 /* p.Ap <= 0 stopped CG */
+#define GGB_SOLVE_MAXIT 8     /* cg_maxit iterations without reaching cg_tol */
+int ggb_solve_flags(const Fluid *F);
+/* Checks the public grid arrays for corruption: non-finite or non-positive
+ * areas, link weights and edge lengths, neighbour counts above 8 and
+ * neighbour indices out of range.  Returns the number of bad entries (0 for
+ * an intact grid).  The solve reads the operator tables built at cs_init,
+ * not these arrays; a caller that edits them can detect it here. */
+long ggb_grid_validate(const CubeSphere *cs);
+/* Host-side fault injection for tests: after `after` more successful device
+ * or managed allocations, every allocation of the library fails as if device
+ * memory were exhausted (no allocator call is made); after < 0 turns it off.
+ * cs_init, particles_init and render_init then return -1 with a message and
+ * release what they had allocated (upstream's convention for these three);
+ * other entry points end the process, as upstream does on OOM. */
+void ggb_inject_alloc_failure(long after);
 /* The next solves record up to `cap` (mark, nanoseconds) pairs of their phase
  * schedule (cap = 0: off); ggb_solve_trace copies them out, returns the count. */
 void ggb_solve_trace_enable(int cap);
@@ -85,12 +114,26 @@ void ggb_taps_batch(const CubeSphere *cs, const double *dirs, int n, int *idx, d
  * Removes the area-weighted mean of f[ncells] in place; f must already be
  * device or managed memory.  Its scratch is one fixed 32 KB device array per
  * GPU (held until the process exits), which limits grids to 16,777,216 cells
- * (N <= 1672); larger grids, host buffers or a failed set-up return -1 with a
- * message and leave f unchanged, success returns 0.  The first call on a
- * device looks up the array's device address (once per device); make that
- * first call before any stream capture.  All calls share the array, so calls
- * whose GPU work overlaps (from several host threads) race. */
+ * (N <= 1672).  Returns 0 on success.  Returns -1 with a message, f unchanged,
+ * when the grid is unknown or larger than that, f is a host buffer, the
+ * current device is not the one of the grid and the library stream, or the
+ * scratch address cannot be looked up; -1 with f undefined when a launch or
+ * the final synchronisation fails.  The first call on a device looks up the
+ * array's device address (once per device).  Every call synchronises the
+ * library stream before it returns, so it must not be called while that
+ * stream is being captured.  All calls share the array, so calls whose GPU
+ * work overlaps (from several host threads) race. */
 int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f);
+
+/* Precision of F's Poisson solve.  mixed = 0 (the default): FP32 vectors with
+ * FP64 stencil accumulation and the upstream CG.  mixed = 1: the multigrid
+ * V-cycle stores its level vectors and the coarse levels' slot weights in
+ * FP16 and accumulates in FP32, inside a flexible (Polak-Ribiere) FP32 CG;
+ * psi, omega and u stay FP32, and the CG dots, the residual norm and the
+ * zero-mean projections stay FP64.  Returns 0, or -1 when F has no multigrid
+ * preconditioner.  The FluidParams layout of the upstream header is kept, so
+ * the choice is made here rather than there. */
+int ggb_fluid_set_precision(Fluid *F, int mixed);
 
 /* Checkpoint / resume of a running planet.  save writes the state the next
  * steps read (omega, omega_band, psi, vel and the last solve's statistics; the

@@ -6,7 +6,7 @@
  * helper header (src/vec3.h:7-58 of gaseous-gusty-ball), because callers
  * compiled against either header must compute identical bits; the bodies
  * are written for this library.  Device code uses its own double3 helpers
- * (gaseous-gusty-ball_b200/csrc/ggb_math.cuh) with the same expression order.
+ * (gaseous-gusty-ball_b200/csrc/ggb_device.cuh) with the same expression order.
  */
 #ifndef GGB_VEC3_H
 #define GGB_VEC3_H

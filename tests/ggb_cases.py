@@ -87,10 +87,10 @@ def operators(api, N):
     return dict(lap=y, curl=curl, div=div, mean_removed=f)
 
 
-def poisson(api, N, tol=1e-6, maxit=5000):
+def poisson(api, N, tol=1e-6, maxit=5000, mixed=False):
     """upstream tests/test_poisson.c:51-72: solve Laplacian(psi) = lap_exact."""
     g = api.grid(N)
-    fs = G.FluidSim(api, g, cg_tol=tol, cg_maxit=maxit)
+    fs = G.FluidSim(api, g, cg_tol=tol, cg_maxit=maxit, mixed=mixed)
     pos = g.arrays()["pos"].astype(np.float64)
     om = fs.field("omega")
     om[:] = lap_exact(pos).astype(api.np_real)
@@ -117,11 +117,13 @@ def initial_velocity(api, g, seed=1, bands=8):
 
 
 def run(api, N, particles, R, steps, vel0, vband, forcing=0.5, rotation=3.0, tol=1e-6, fixed_dt=0.0,
-        cfl=1.0, fade=0.02, strip_seed=1, bfecc=1):
+        cfl=1.0, fade=0.02, strip_seed=1, bfecc=1, snaps=(), dts_in=None, maxit=500, mixed=False):
     """The application driver's step loop (upstream src/main.c:421-438):
-    dt from CFL, particles_advect, fluid_step, render_fade, render_deposit."""
+    dt from CFL, particles_advect, fluid_step, render_fade, render_deposit.
+    snaps: steps after which the state is recorded in out["snap"][step];
+    dts_in: the time step of every step (instead of the CFL step)."""
     g = api.grid(N)
-    fs = G.FluidSim(api, g, forcing=forcing, rotation=rotation, cg_tol=tol, bfecc=bfecc)
+    fs = G.FluidSim(api, g, forcing=forcing, rotation=rotation, cg_tol=tol, bfecc=bfecc, cg_maxit=maxit, mixed=mixed)
     nr = api.np_real
     fs.set_state(np.asarray(vel0, nr), None if vband is None else np.asarray(vband, nr))
     out = dict(omega0=fs.field("omega").copy(), psi0=fs.field("psi").copy(), vel0=fs.field("vel", 3).copy(),
@@ -131,9 +133,13 @@ def run(api, N, particles, R, steps, vel0, vband, forcing=0.5, rotation=3.0, tol
     out["col"] = ps.array("col", 4).copy()
     sp = G.Splat(api, R)
     dts, cgs = [], []
+    if snaps:
+        out["snap"] = {}
     for s in range(steps):
         dt = fixed_dt
-        if dt <= 0:
+        if dts_in is not None:
+            dt = float(dts_in[s])
+        elif dt <= 0:
             vmax = fs.max_speed()
             dt = cfl * g.cs.h / (vmax if vmax > 1e-6 else 1e-6)
         ps.advect(g, fs.F.vel, dt)
@@ -142,6 +148,10 @@ def run(api, N, particles, R, steps, vel0, vband, forcing=0.5, rotation=3.0, tol
         sp.deposit(ps)
         dts.append(dt)
         cgs.append(fs.F.cg_iters)
+        if s + 1 in snaps:
+            out["snap"][s + 1] = dict(omega=fs.field("omega").copy(), psi=fs.field("psi").copy(),
+                                      vel=fs.field("vel", 3).copy(), pos=ps.array("pos", 3).copy(),
+                                      faces=sp.faces())
     out.update(omega=fs.field("omega").copy(), psi=fs.field("psi").copy(), vel=fs.field("vel", 3).copy(),
                pos=ps.array("pos", 3).copy(), prev=ps.array("prev", 3).copy(), faces=sp.faces(),
                dts=np.array(dts), cg=np.array(cgs), g=np.array(sp.r.g))

@@ -14,7 +14,21 @@ import ggb_api
 from conftest import ROOT
 
 INCLUDE = os.path.join(ROOT, "include")
-UPSTREAM_SRC = "/root/reference/src"
+
+
+def _upstream_src():
+    """The upstream header directory: $GGB_UPSTREAM_SRC, else the one that
+    oracle/Makefile recorded when it built the upstream sources (None when
+    neither exists, e.g. on a machine without the upstream sources)."""
+    p = os.environ.get("GGB_UPSTREAM_SRC")
+    if not p:
+        rec = os.path.join(ROOT, "oracle", "_ref", "upstream_src.path")
+        if os.path.exists(rec):
+            p = open(rec).read().strip()
+    return p if p and os.path.isdir(p) else None
+
+
+UPSTREAM_SRC = _upstream_src()
 
 
 def _strip_bodies(text):
@@ -128,6 +142,7 @@ def test_struct_layouts_match_ctypes(tmp_path):
     assert int(lines["Fluid.cg_relres"]) == T["Fluid"].cg_relres.offset
 
 
-@pytest.mark.skipif(not os.path.isdir(UPSTREAM_SRC), reason="upstream headers not present on this machine")
+@pytest.mark.skipif(UPSTREAM_SRC is None, reason="upstream headers not present on this machine "
+                                                 "(set GGB_UPSTREAM_SRC or build oracle/_ref)")
 def test_struct_layouts_match_upstream_headers(tmp_path):
     assert _layout(tmp_path, INCLUDE, "inc") == _layout(tmp_path, UPSTREAM_SRC, "up")

@@ -16,10 +16,17 @@ import ggb_cases as K
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_mean_removal_matches_fluid_remove_mean(gpu):
+def _bind(gpu):
     gpu.lib.ggb_remove_mean_noalloc.restype = C.c_int
     gpu.lib.ggb_remove_mean_noalloc.argtypes = [C.POINTER(gpu.T["CubeSphere"]), C.POINTER(C.c_float)]
-    g = gpu.grid(64)
+
+
+# N=64: 24,576 cells, exactly six 4096-cell blocks; N=50: 15,000 cells, whose
+# last block is partial (its cell range is clamped to the grid)
+@pytest.mark.parametrize("N", [64, 50])
+def test_noalloc_mean_removal_matches_fluid_remove_mean(gpu, N):
+    _bind(gpu)
+    g = gpu.grid(N)
     fs = G.FluidSim(gpu, g)  # two device-resident (managed) buffers of ncells floats
     a, b = fs.field("omega"), fs.field("psi")
     pos = g.arrays()["pos"].astype(np.float64)
@@ -34,4 +41,17 @@ def test_noalloc_mean_removal_matches_fluid_remove_mean(gpu):
         assert np.max(np.abs(a.astype(np.float64) - b)) <= 1e-6 * np.max(np.abs(field)), f"call {call}"
         assert abs(float(np.sum(g.arrays()["area"].astype(np.float64) * b))) < 1e-5
     fs.free()
+    g.free()
+
+
+def test_noalloc_rejects_host_buffers(gpu):
+    """A pageable host array would need a staging allocation: the entry point
+    refuses it with -1 and leaves it untouched."""
+    _bind(gpu)
+    g = gpu.grid(16)
+    f = np.linspace(1.0, 2.0, g.n).astype(np.float32)
+    keep = f.copy()
+    rc = gpu.lib.ggb_remove_mean_noalloc(C.byref(g.cs), f.ctypes.data_as(C.POINTER(C.c_float)))
+    assert rc == -1
+    assert np.array_equal(f, keep)
     g.free()
