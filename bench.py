@@ -58,11 +58,10 @@ def args_():
     p.add_argument("--workload", choices=["default", "large", "batch"], default="default",
                    help="large: N=512, 4M particles, 2048^2 faces, forcing 0.5, rotation 10; "
                         "batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping")
-    p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
+    p.add_argument("--precision", choices=["plain", "mixed"], default=None,
                    help="plain: FP32 solve with FP64 stencil sums; mixed: FP16 V-cycle storage, FP32 accumulation, "
-                        "flexible CG (FP64 dots and mean projections in both)")
-    p.add_argument("--cells-per-block", type=int, default=0,
-                   help="batch: cells per block of the batched solves (0: tune over a few candidates)")
+                        "flexible CG (FP64 dots and mean projections in both).  Default: plain, except mixed for "
+                        "--workload batch")
     return p.parse_args()
 
 
@@ -500,12 +499,65 @@ def batch_specs(count=64, seed=7):
     return out
 
 
+def batch_fp64_check(planets, count=4):
+    """psi / u of the last batched solves against the FP64 upstream build
+    solving the same omega to relative residual 1e-10 (a few planets, one of
+    each grid size first); part of the batch's ``cpu_baseline`` leg."""
+    path64 = os.path.join(ROOT, "oracle", "_ref", "libggbref64.so")
+    if not os.path.exists(path64):
+        return None
+    ref = G.Api(path64, C.c_double)
+    ref.lib.drv_set_threads(os.cpu_count())
+    seen, pick = set(), []
+    for k, p in enumerate(planets):
+        if p[4]["N"] not in seen:
+            seen.add(p[4]["N"])
+            pick.append(k)
+    pick += [k for k in range(len(planets)) if k not in pick][:max(0, count - len(pick))]
+    rel = lambda x, y: float(np.linalg.norm(np.asarray(x, np.float64) - y) / np.linalg.norm(y))
+    worst_psi = worst_u = 0.0
+    rows = []
+    for k in pick:
+        g, fs, ps, spl, sp = planets[k]
+        go = ref.grid(sp["N"])
+        f64 = G.FluidSim(ref, go, cg_tol=1e-10, cg_maxit=5000)
+        f64.field("omega")[:] = fs.field("omega").astype(np.float64)
+        ref.lib.fluid_remove_mean(C.byref(go.cs), f64.F.omega)
+        ref.lib.fluid_solve_psi(C.byref(f64.F))
+        ref.lib.fluid_compute_velocity(C.byref(f64.F))
+        e_psi, e_u = rel(fs.field("psi"), f64.field("psi")), rel(fs.field("vel", 3), f64.field("vel", 3))
+        rows.append({"planet": k, "N": sp["N"], "psi_rel_l2": e_psi, "u_rel_l2": e_u})
+        worst_psi, worst_u = max(worst_psi, e_psi), max(worst_u, e_u)
+        f64.free()
+        go.free()
+    return {"psi_rel_l2_max": worst_psi, "u_rel_l2_max": worst_u, "planets": rows,
+            "reference": "upstream sources built with -Dfloat=double solving each planet's final omega (after the "
+                         "timed steps and one more batched step) to relative residual 1e-10"}
+
+
+def batch_cpu_baseline(spec, steps=3):
+    """The upstream FP64 build on one planet of the batch (its first N=256
+    planet): the CPU reference's planet-steps/s."""
+    path64 = os.path.join(ROOT, "oracle", "_ref", "libggbref64.so")
+    if not os.path.exists(path64):
+        return None
+    phys, logical = host_cores()
+    pl, dt, its = _time_ref(path64, C.c_double, spec, steps, logical)
+    pl.free()
+    return dict(value=steps / dt, unit="planet-steps/s", cores=logical, physical_cores=phys, logical_cpus=logical,
+                kind="reference",
+                sample=f"{steps} steps of one N={spec['N']} planet of the batch ({spec['particles']} particles, "
+                       f"{spec['R']}^2 faces) after 1 warm-up step, upstream FP64 build, {logical} OpenMP threads")
+
+
 def run_batch(a, rank, world, local):
-    """64 uneven planets advanced by ggb_batch_step, against the same planets
-    stepped one after another through the per-planet entry points.  With N
-    ranks every rank takes its share of the planets (longest processing time
-    first by estimated cost, ggb_shard.assign); no collective on the data
-    path, the job time is the maximum over ranks."""
+    """64 uneven planets advanced by ggb_batch_step (one persistent solve
+    launch for all planets with autotuned shares; mixed precision unless
+    --precision plain), against the same planets stepped one after another
+    through the per-planet entry points in the plain FP32 form.  With N ranks
+    every rank takes its share of the planets (longest processing time first
+    by estimated cost, ggb_shard.assign); no collective on the data path, the
+    job time is the maximum over ranks."""
     import torch
     import ggb_shard
     dist = None
@@ -517,6 +569,10 @@ def run_batch(a, rank, world, local):
     api = G.Api(G.PRODUCT_LIB)
     if api.lib.ggb_set_device(local) != 0:
         raise RuntimeError(f"cannot select CUDA device {local}")
+    for name, res, args in (("ggb_timer_start", None, []), ("ggb_timer_stop", C.c_double, [])):
+        fn = getattr(api.lib, name)
+        fn.restype, fn.argtypes = res, args
+    mixed = a.precision != "plain"
 
     def barrier():
         if dist:
@@ -540,7 +596,7 @@ def run_batch(a, rank, world, local):
         vb = np.zeros(3 * g.n, api.np_real)
         api.lib.ggb_initial_velocity(C.byref(g.cs), C.byref(ip), api.ptr(vel), api.ptr(vb))
         fs = G.FluidSim(api, g, forcing=sp["forcing"], rotation=sp["rotation"], cg_tol=sp["cg_tol"],
-                        cg_maxit=sp["cg_maxit"])
+                        cg_maxit=sp["cg_maxit"], mixed=mixed)
         fs.set_state(vel, vb if sp["forcing"] > 0 else None)
         ps = G.ParticleSet(api, sp["particles"])
         ps.colour(ggb_inputs.strip(sp["seed"]))
@@ -555,18 +611,12 @@ def run_batch(a, rank, world, local):
     fd = (C.c_double * n)(*[p[4]["fade"] for p in planets])
     b = api.lib.ggb_batch_create(n, Fs, Ps, Rs, cf, fd)
     K = min(a.steps, 20)
-    W = max(3, min(a.warmup, 5))
+    W = max(5, min(a.warmup, 8))  # the library's autotuner refines its shares over the first steps
     api.lib.ggb_batch_step(b, W)
-    # tuning: the solve grid granularity, timed over two batched steps each
-    tried = {}
-    for cpb in ([a.cells_per_block] if a.cells_per_block > 0 else [4096, 8192, 16384, 32768, 65536]):
-        api.lib.ggb_batch_cells_per_block(b, cpb)
-        api.lib.ggb_batch_step(b, 1)
-        t1 = time.perf_counter()
-        api.lib.ggb_batch_step(b, 2)
-        tried[cpb] = (time.perf_counter() - t1) / 2 * 1000
-    best = min(tried, key=tried.get)
-    api.lib.ggb_batch_cells_per_block(b, best)
+
+    def set_precision(m):
+        for p in planets:
+            api.lib.ggb_fluid_set_precision(C.byref(p[1].F), int(m))
 
     def plain_step(p):
         g, fs, ps, spl, sp = p
@@ -578,6 +628,7 @@ def run_batch(a, rank, world, local):
         lib.render_fade(C.byref(spl.r), sp["fade"])
         lib.render_deposit(C.byref(spl.r), C.byref(ps.P))
 
+    set_precision(False)
     for p in planets:  # plain warm-up
         plain_step(p)
     # batched and plain segments alternate on the same evolving planets (the
@@ -585,15 +636,21 @@ def run_batch(a, rank, world, local):
     clk, clk_path = start_clock_sampler(local)
     time.sleep(0.3)
     ms_b = ms_p = 0.0
-    its = []
+    its, solve_ms = [], []
     half = max(1, K // 2)
+    launches_b = 0
     for seg in range(2):
+        set_precision(mixed)
         barrier()
+        lb = api.lib.ggb_launch_count()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
         api.lib.ggb_batch_step(b, half)
         ms_b += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
+        launches_b += api.lib.ggb_launch_count() - lb
         its += [p[1].F.cg_iters for p in planets]
+        solve_ms.append(api.lib.ggb_batch_solve_ms(b))
+        set_precision(False)
         barrier()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
@@ -603,32 +660,53 @@ def run_batch(a, rank, world, local):
         ms_p += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
     clocks = stop_clock_sampler(clk, clk_path)
     K = 2 * half
+    # one more batched step: the state the FP64 check below solves again
+    set_precision(mixed)
+    api.lib.ggb_batch_step(b, 1)
     wq, cq = C.c_double(), C.c_double()
     host_enq = api.lib.ggb_batch_host_ms(b, C.byref(wq), C.byref(cq))
     host_ms = {"enqueue": host_enq, "gpu_wait": wq.value, "collect": cq.value}
-    api.lib.ggb_batch_free(b)
+    blocks = (C.c_int * n)()
+    api.lib.ggb_batch_blocks(b, blocks)
+    shares = {}
+    for p, nb in zip(planets, blocks):
+        shares.setdefault(str(p[4]["N"]), []).append(int(nb))
+    tuned = {str(N): api.lib.ggb_batch_cost(N, int(mixed)) for N in (64, 128, 256)}
     cells = sum(6 * p["N"] ** 2 for p in all_specs)
     parts = sum(p["particles"] for p in all_specs)
     value = len(all_specs) * K / (ms_b / 1000.0)
     plain = len(all_specs) * K / (ms_p / 1000.0)
+    base = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        first256 = next((p[4] for p in planets if p[4]["N"] == 256), planets[0][4])
+        base = batch_cpu_baseline(first256)
+        if base is not None:
+            base["fp64_error"] = batch_fp64_check(planets)
+    api.lib.ggb_batch_free(b)
     if rank == 0:
         print(json.dumps({
             "metric": "planet-steps/s (64 uneven planets, batched)", "value": value, "unit": "planet-steps/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_b / K, "higher_is_better": True,
-            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "f32+f16" if mixed else "f32", "data": "synthetic",
             "plain": {"value": plain, "unit": "planet-steps/s", "ms_per_step": ms_p / K,
-                      "note": "the same planets, each stepped through the per-planet entry points in turn"},
+                      "note": "the same planets, each stepped through the per-planet entry points in turn, "
+                              "plain FP32 solve"},
             "speedup_vs_plain": value / plain,
             "config": {"workload": "64 planets, N uniform in {64,128,256}, particles uniform in [100k,1M], faces "
                                    "512^2 or 1024^2, bands in {4,8,12}, noise scale in [2,5], PCG tol 1e-6, CFL 1",
                        "planets_by_N": {str(k): sum(1 for p in all_specs if p["N"] == k) for k in (64, 128, 256)},
                        "parallelism": f"batch sharded over {world} GPU(s) by estimated planet cost (LPT)",
+                       "precision": "mixed (FP16 V-cycle, flexible CG) batched vs plain FP32 per-planet" if mixed
+                                    else "plain FP32 in both",
                        "cells": cells, "particles": parts, "mean_cg_iters": float(np.mean(its)),
-                       "psi_error": "batched and plain run the same FP32 solve to the same tolerance",
-                       "cells_per_block": best, "tuning_ms_per_step": {str(k): v for k, v in tried.items()},
+                       "solve_blocks_by_N": shares, "tuned_cost_s_per_cell_block": tuned,
+                       "batched_solve_ms_last_step": solve_ms,
                        "host_ms_last_step": host_ms,
                        "deposit_repeats": int(sum(api.lib.ggb_render_repeats(C.byref(p[3].r)) for p in planets)),
                        "timing": "max of CUDA events on the library stream and the host wall clock"},
+            "cpu_baseline": base,
+            "gpu_launches": int(launches_b),
             "clocks": clocks}), flush=True)
     for g, fs, ps, spl, sp in planets:
         spl.free()

@@ -4,27 +4,70 @@
 // render_init; grids may be shared between planets of the same N).  One
 // batched step is the application driver's step for every planet (upstream
 // src/main.c:421-434: CFL dt from the maximum speed, particles_advect,
-// fluid_step, render_fade, render_deposit), with three differences from
+// fluid_step, render_fade, render_deposit), with these differences from
 // calling those entry points planet after planet:
-//   - each planet's work is queued on its own stream, so the kernels of
-//     different planets overlap on the GPU;
-//   - the CFL dt is computed on the device (same expression, same IEEE
-//     square root and division as the driver, so the same dt), so nothing
-//     returns to the host inside a step;
-//   - a planet's solve runs on a grid proportional to its size (one block
-//     per `cells_per_block` cells, at most one per SM), so small planets take
-//     a share of the SMs and several solves run at once.
+//   - the Poisson solves of all planets run in ONE persistent cooperative
+//     launch: every planet gets a share of the resident blocks and runs its
+//     solve on them with its own barrier, reductions and convergence test, so
+//     a small planet's solve is not a whole-GPU launch that waits on its own
+//     latency, and the planets' solves fill the GPU together;
+//   - the shares are chosen by an autotuner that this file implements: each
+//     solve reports its device time, from which a cost per cell and block is
+//     estimated for every grid size (and precision); blocks are then given out
+//     so that the estimated finishing times are equal (the largest finishing
+//     time is minimised under the launch's capacity).  The estimates are kept
+//     per grid size for the life of the process, so a later batch with the
+//     same grid sizes starts from them;
+//   - the work before and after the solve (CFL dt, particle advection, the
+//     BFECC advection; velocity, fade and splat) is queued on one stream per
+//     planet, so the kernels of different planets overlap;
+//   - the CFL dt is computed on the device (same expression, same IEEE square
+//     root and division as the driver, so the same dt), so nothing returns to
+//     the host inside a step.
 // The host synchronises once per batched step, then reads each solve's
 // statistics and checks each deposit's record buffer (growing it and
 // repeating that planet's compositing in the rare step where it was short).
-// Results equal the per-planet entry points' up to the relaxation factor of
-// the forcing, 1 - exp(-forcing dt), which the device computes with its own
-// exp (last-bit differences).
+// Planets of the two precisions are solved in separate batched launches, as
+// are planets beyond what one launch can hold.
+// Results equal the per-planet entry points' up to the order of the solve's
+// FP64 block sums (another number of blocks) and the device's exp in the
+// forcing's relaxation factor, 1 - exp(-forcing dt).
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "ggb_internal.h"
+#include "ggb_solver.h"
+
+using namespace ggb;
+
+namespace {
+
+// Tuned cost of a solve: device seconds per cell for one block, per (grid N,
+// precision); shared by all batches of the process.
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, double> g_cost;
+
+double cost_of(int N, int mixed) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_cost.find({N, mixed});
+    return it == g_cost.end() ? 0.0 : it->second;
+}
+
+void cost_update(int N, int mixed, double c) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_cost.find({N, mixed});
+    if (it == g_cost.end())
+        g_cost[{N, mixed}] = c;
+    else
+        it->second = 0.5 * (it->second + c);  // smooth over steps
+}
+
+}  // namespace
 
 struct GGBBatch {
     int n = 0;
@@ -33,13 +76,158 @@ struct GGBBatch {
     std::vector<Render *> r;
     std::vector<double> cfl, fade;
     std::vector<cudaStream_t> st;
+    std::vector<cudaEvent_t> ev_pre;
     double *dt_dev = nullptr;  // [n] device-side time steps
-    int cells_per_block = 2048;
-    cudaEvent_t fork = nullptr;
+    cudaEvent_t fork = nullptr, ev_solve = nullptr;
+    // the batched solve
+    GridBarrier *bars = nullptr;          // [n] one barrier per planet (zeroed before each launch)
+    SolveParams *prm_host = nullptr;      // [n] pinned
+    SolveParams *prm_dev = nullptr;       // [n]
+    std::vector<std::vector<int>> groups;  // planets of each launch
+    std::vector<size_t> group_smem;        // dynamic shared memory of each launch
+    std::vector<int> blocks;               // blocks of each planet's solve
+    int4 *bmap_host = nullptr, *bmap_dev = nullptr;  // [sum of blocks] block -> (planet, block, blocks)
+    int bmap_cap = 0;
+    int tune_steps = 0;     // batched steps over which the cost estimates are refined
+    int fixed_blocks = 0;   // > 0: every planet's solve gets this many blocks (no tuning)
     double enqueue_ms = 0, wait_ms = 0, collect_ms = 0;  // host time of the last step's three parts
+    double solve_ms = 0;  // device time of the last step's slowest planet solve
 };
 
-using namespace ggb;
+static int n_cells(const GGBBatch *b, int i) { return b->F[i]->cs->ncells; }
+static int grid_n(const GGBBatch *b, int i) { return b->F[i]->cs->N; }
+
+// Blocks per planet of one launch: minimise the largest estimated finishing
+// time  cost(N_i) * cells_i / blocks_i  with sum blocks_i <= cap, blocks_i >= 1
+// (binary search on the finishing time).  Unknown costs count as the
+// smallest known cost of that precision (or 1), which makes the first split
+// proportional to the planets' cells.
+static void allocate(GGBBatch *b, const std::vector<int> &grp, int cap) {
+    const int mixed = fluid_solve_mixed(b->F[grp[0]]);
+    std::vector<double> w(grp.size());
+    double known = 0;
+    for (size_t k = 0; k < grp.size(); k++) {
+        double c = cost_of(grid_n(b, grp[k]), mixed);
+        if (c > 0) known = known > 0 ? std::min(known, c) : c;
+    }
+    for (size_t k = 0; k < grp.size(); k++) {
+        double c = cost_of(grid_n(b, grp[k]), mixed);
+        w[k] = (c > 0 ? c : (known > 0 ? known : 1.0)) * n_cells(b, grp[k]);
+    }
+    auto need = [&](double T) {
+        long s = 0;
+        for (size_t k = 0; k < grp.size(); k++) s += std::max(1L, (long)std::ceil(w[k] / T));
+        return s;
+    };
+    double lo = 0, hi = *std::max_element(w.begin(), w.end());  // at T = hi every planet needs 1 block
+    for (int it = 0; it < 60; it++) {
+        double mid = 0.5 * (lo + hi);
+        if (need(mid) <= cap)
+            hi = mid;
+        else
+            lo = mid;
+    }
+    long used = 0;
+    for (size_t k = 0; k < grp.size(); k++) {
+        b->blocks[grp[k]] = std::max(1, (int)std::ceil(w[k] / hi));
+        used += b->blocks[grp[k]];
+    }
+    // blocks left over go to the planets with the largest time per block (a
+    // planet never gets more than one block per 512 cells)
+    while (used < cap) {
+        long best = -1;
+        double bt = -1;
+        for (size_t k = 0; k < grp.size(); k++) {
+            if ((long)b->blocks[grp[k]] * 512 >= n_cells(b, grp[k])) continue;
+            const double t = w[k] / b->blocks[grp[k]];
+            if (t > bt) {
+                bt = t;
+                best = (long)k;
+            }
+        }
+        if (best < 0) break;
+        b->blocks[grp[best]]++;
+        used++;
+    }
+}
+
+// Launch groups (planets of one precision, at most cap of them each), block
+// shares and the block map.
+static void plan(GGBBatch *b) {
+    b->groups.clear();
+    b->group_smem.clear();
+    b->blocks.assign(b->n, 1);
+    std::vector<int> order[2];
+    for (int i = 0; i < b->n; i++) order[fluid_solve_mixed(b->F[i])].push_back(i);
+    int total = 0;
+    for (int m = 0; m < 2; m++) {
+        if (order[m].empty()) continue;
+        // the launch's shared memory: the largest of its planets' needs
+        size_t smem = 0;
+        for (int i : order[m]) smem = std::max(smem, pcg_launch_smem(b->prm_host[i]));
+        const int cap = pcg_batch_capacity(smem, m == 1);
+        if (b->fixed_blocks >= cap) {
+            // every planet alone on the whole launch: one launch per planet,
+            // the same blocks (and so the same arithmetic) as fluid_step's solve
+            for (int i : order[m]) {
+                b->blocks[i] = cap;
+                total += cap;
+                b->groups.push_back(std::vector<int>{i});
+                b->group_smem.push_back(smem);
+            }
+            continue;
+        }
+        for (size_t k0 = 0; k0 < order[m].size(); k0 += cap) {
+            std::vector<int> grp(order[m].begin() + k0,
+                                 order[m].begin() + std::min(order[m].size(), k0 + (size_t)cap));
+            if (b->fixed_blocks > 0) {
+                // a fixed share, scaled down when the launch cannot hold it
+                const int per = std::max(1, std::min(b->fixed_blocks, cap / (int)grp.size()));
+                for (int i : grp) b->blocks[i] = per;
+            } else {
+                allocate(b, grp, cap);
+            }
+            for (int i : grp) total += b->blocks[i];
+            b->groups.push_back(grp);
+            b->group_smem.push_back(smem);
+        }
+    }
+    if (total > b->bmap_cap) {
+        cudaFreeHost(b->bmap_host);
+        dev_free(b->bmap_dev);
+        GGB_CHECK(cudaMallocHost(&b->bmap_host, sizeof(int4) * total));
+        b->bmap_dev = (int4 *)dev_alloc(sizeof(int4) * total);
+        b->bmap_cap = total;
+    }
+    int q = 0;
+    for (auto &grp : b->groups)
+        for (int i : grp)
+            for (int k = 0; k < b->blocks[i]; k++) b->bmap_host[q++] = make_int4(i, k, b->blocks[i], 0);
+    GGB_CHECK(cudaMemcpyAsync(b->bmap_dev, b->bmap_host, sizeof(int4) * total, cudaMemcpyHostToDevice, stream()));
+}
+
+// The planets' solve parameters (they hold the planets' buffers, which do not
+// move, and the precision, which ggb_fluid_set_precision may change).
+static void refresh_params(GGBBatch *b) {
+    sync();  // the pinned parameter and block-map buffers may still be in use by queued copies
+    for (int i = 0; i < b->n; i++) fluid_step_solve_params(b->F[i], b->bars + i, b->prm_host + i);
+    GGB_CHECK(cudaMemcpyAsync(b->prm_dev, b->prm_host, sizeof(SolveParams) * b->n, cudaMemcpyHostToDevice,
+                              stream()));
+    plan(b);
+}
+
+// Cost estimates from the last step's solve times.
+static void tune(GGBBatch *b) {
+    std::map<std::pair<int, int>, std::pair<double, int>> acc;
+    for (int i = 0; i < b->n; i++) {
+        const double t = fluid_last_solve_seconds(b->F[i]);
+        if (t <= 0) continue;
+        auto &a = acc[{grid_n(b, i), fluid_solve_mixed(b->F[i])}];
+        a.first += t * b->blocks[i] / n_cells(b, i);
+        a.second++;
+    }
+    for (auto &kv : acc) cost_update(kv.first.first, kv.first.second, kv.second.first / kv.second.second);
+}
 
 GGB_EXPORT GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *P, Render *const *r,
                                       const double *cfl, const double *fade) {
@@ -65,17 +253,32 @@ GGB_EXPORT GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *
         cudaStream_t s;
         GGB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         b->st.push_back(s);
+        cudaEvent_t e;
+        GGB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->ev_pre.push_back(e);
     }
     b->dt_dev = (double *)dev_alloc(sizeof(double) * n);
+    b->bars = (GridBarrier *)dev_alloc(sizeof(GridBarrier) * n);
+    GGB_CHECK(cudaMallocHost(&b->prm_host, sizeof(SolveParams) * n));
+    b->prm_dev = (SolveParams *)dev_alloc(sizeof(SolveParams) * n);
     GGB_CHECK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    GGB_CHECK(cudaEventCreateWithFlags(&b->ev_solve, cudaEventDisableTiming));
+    b->tune_steps = 4;
     sync();
     return b;
 }
 
-// Cells per block of the batched solves (default 2048); returns the value in use.
-GGB_EXPORT int ggb_batch_cells_per_block(GGBBatch *b, int cells) {
-    if (cells > 0) b->cells_per_block = cells;
-    return b->cells_per_block;
+// Fixed blocks per planet solve (blocks > 0: that many for every planet,
+// without tuning, and at or above the launch's capacity one launch per planet
+// on all of it; 0: the autotuned shares; < 0: query).  Returns the setting.
+GGB_EXPORT int ggb_batch_solve_blocks(GGBBatch *b, int blocks) {
+    if (blocks >= 0) b->fixed_blocks = blocks;
+    return b->fixed_blocks;
+}
+
+// The blocks each planet's solve ran on in the last step (host array of n).
+GGB_EXPORT void ggb_batch_blocks(const GGBBatch *b, int *blocks) {
+    for (int i = 0; i < b->n; i++) blocks[i] = (int)b->blocks.size() > i ? b->blocks[i] : 0;
 }
 
 // The time steps of the last batched step (host array of n).
@@ -87,6 +290,7 @@ GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
     if (!b) return -1;
     const cudaStream_t base = stream();
     using clk = std::chrono::steady_clock;
+    refresh_params(b);
     for (int k = 0; k < steps; k++) {
         const auto t0 = clk::now();
         // every planet's stream starts after the work already queued on the library stream
@@ -95,24 +299,52 @@ GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
             GGB_CHECK(cudaStreamWaitEvent(b->st[i], b->fork, 0));
             set_stream(b->st[i]);
             Fluid *F = b->F[i];
-            const int blocks = (F->cs->ncells + b->cells_per_block - 1) / b->cells_per_block;
             fluid_cfl_dt_launch(F, b->cfl[i], b->dt_dev + i);
             if (b->P[i]) particles_advect_queue(b->P[i], F->cs, F->vel, b->dt_dev + i);
-            fluid_step_queue(F, b->dt_dev + i, blocks);
+            fluid_advect_queue(F, b->dt_dev + i);
+            GGB_CHECK(cudaEventRecord(b->ev_pre[i], b->st[i]));
+        }
+        set_stream(nullptr);
+        // the batched solves, on the library stream after every planet's advection
+        for (int i = 0; i < b->n; i++) GGB_CHECK(cudaStreamWaitEvent(base, b->ev_pre[i], 0));
+        GGB_CHECK(cudaMemsetAsync(b->bars, 0, sizeof(GridBarrier) * b->n, base));
+        int q = 0;
+        for (size_t g = 0; g < b->groups.size(); g++) {
+            const std::vector<int> &grp = b->groups[g];
+            int nb = 0;
+            for (int i : grp) nb += b->blocks[i];
+            pcg_launch_batch(b->prm_dev, b->bmap_dev + q, nb, fluid_solve_mixed(b->F[grp[0]]) != 0, b->group_smem[g],
+                             base);
+            q += nb;
+        }
+        GGB_CHECK(cudaEventRecord(b->ev_solve, base));
+        for (int i = 0; i < b->n; i++) {
+            GGB_CHECK(cudaStreamWaitEvent(b->st[i], b->ev_solve, 0));
+            set_stream(b->st[i]);
+            fluid_result_velocity_queue(b->F[i]);
             if (b->r[i]) {
                 render_fade(b->r[i], b->fade[i]);
                 if (b->P[i]) render_deposit_queue(b->r[i], b->P[i]);
             }
         }
+        set_stream(nullptr);
         const auto t1 = clk::now();
         for (int i = 0; i < b->n; i++) GGB_CHECK(cudaStreamSynchronize(b->st[i]));
         const auto t2 = clk::now();
+        double smax = 0;
         for (int i = 0; i < b->n; i++) {
             set_stream(b->st[i]);
             fluid_step_collect(b->F[i]);
+            smax = std::max(smax, fluid_last_solve_seconds(b->F[i]));
             if (b->r[i] && b->P[i]) render_deposit_collect(b->r[i], b->P[i]);
         }
         set_stream(nullptr);
+        b->solve_ms = 1000 * smax;
+        if (b->fixed_blocks <= 0 && b->tune_steps > 0) {
+            tune(b);
+            b->tune_steps--;
+            plan(b);
+        }
         const auto t3 = clk::now();
         b->enqueue_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
         b->wait_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
@@ -130,13 +362,28 @@ GGB_EXPORT double ggb_batch_host_ms(const GGBBatch *b, double *wait_ms, double *
     return b->enqueue_ms;
 }
 
+// Device time (ms) of the last step's batched solves (the slowest planet's).
+GGB_EXPORT double ggb_batch_solve_ms(const GGBBatch *b) { return b->solve_ms; }
+
+// The autotuner's current cost estimate for grid N (precision mixed): device
+// seconds per cell for one block of the solve; 0 when not measured yet.
+GGB_EXPORT double ggb_batch_cost(int N, int mixed) { return cost_of(N, mixed); }
+
 GGB_EXPORT void ggb_batch_free(GGBBatch *b) {
     if (!b) return;
     for (cudaStream_t s : b->st) {
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
     }
+    sync();
+    for (cudaEvent_t e : b->ev_pre) cudaEventDestroy(e);
     dev_free(b->dt_dev);
+    dev_free(b->bars);
+    dev_free(b->prm_dev);
+    dev_free(b->bmap_dev);
+    cudaFreeHost(b->prm_host);
+    cudaFreeHost(b->bmap_host);
     cudaEventDestroy(b->fork);
+    cudaEventDestroy(b->ev_solve);
     delete b;
 }

@@ -741,10 +741,10 @@ GGB_EXPORT void fluid_set_state(Fluid *F, const float *vel_initial, const float 
     sync();
 }
 
-// upstream src/fluid.c:424-478
-// The body of fluid_step without its synchronisation (dt, or *dtp on the
-// device when dtp is not null; the solve on at most max_blocks blocks when > 0).
-static void step_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp, int max_blocks) {
+// upstream src/fluid.c:424-478, before the solve: departures, BFECC
+// resampling, limiter and relaxation (dt, or *dtp on the device when dtp is
+// not null).
+static void advect_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp) {
     const GridTables *t = Pv->grid0;
     cudaStream_t s = stream();
     double two_omega = 2.0 * F->prm.rotation;
@@ -766,6 +766,12 @@ static void step_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp, i
                                     F->omega_band, F->q1, F->omega);
     GGB_LAUNCHED();
     stage_end(ST_ADVECT);
+}
+
+// The body of fluid_step without its synchronisation (the solve on at most
+// max_blocks blocks when > 0).
+static void step_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp, int max_blocks) {
+    advect_launch(F, Pv, dt, dtp);
     solve_launch(F, Pv, 1, F->prm.cg_maxit, max_blocks);
     launch_velocity(F, Pv);
 }
@@ -797,6 +803,28 @@ void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks) {
 }
 
 void fluid_step_collect(Fluid *F) { solve_collect(F, priv_of(F)); }
+
+// The batched step around one batched solve launch: fluid_advect_queue, then
+// the solve (its parameters from fluid_step_solve_params; bar: the barrier the
+// batched launch gives this planet), then fluid_result_velocity_queue.
+void fluid_advect_queue(Fluid *F, const double *dt_dev) { advect_launch(F, priv_of(F), 0.0, dt_dev); }
+
+void fluid_step_solve_params(Fluid *F, GridBarrier *bar, SolveParams *out) {
+    FluidPriv *Pv = priv_of(F);
+    *out = solve_params(F, Pv, 1, F->prm.cg_maxit);
+    out->bar = bar;
+}
+
+int fluid_solve_mixed(const Fluid *F) { return priv_of(F)->mixed; }
+
+// Device time of F's last collected solve, in seconds.
+double fluid_last_solve_seconds(const Fluid *F) { return 1e-9 * (double)priv_of(F)->res_host->ns; }
+
+void fluid_result_velocity_queue(Fluid *F) {
+    FluidPriv *Pv = priv_of(F);
+    GGB_CHECK(cudaMemcpyAsync(Pv->res_host, Pv->res, sizeof(SolveResult), cudaMemcpyDeviceToHost, stream()));
+    launch_velocity(F, Pv);
+}
 
 }  // namespace ggb
 

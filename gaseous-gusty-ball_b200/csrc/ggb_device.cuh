@@ -249,11 +249,12 @@ __device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, un
 // multiple of the number of blocks, which the waiters poll with acquire loads.
 // The arrival is the first global access of a barrier (no generation or error
 // read before it); the error flag and the timeout are checked every 64 polls.
-__device__ __forceinline__ bool grid_sync_limit(GridBarrier *bar, unsigned long long limit_ns) {
+// nb: the number of blocks that meet at this barrier (the whole grid, or the
+// blocks of one solve inside a batched launch).
+__device__ __forceinline__ bool grid_sync_nb(GridBarrier *bar, unsigned int nb, unsigned long long limit_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
         const unsigned int old = atom_add_acq_rel_u32(&bar->count, 1u);
         const unsigned int target = (old / nb + 1u) * nb;
         int ok = 1;
@@ -279,6 +280,9 @@ __device__ __forceinline__ bool grid_sync_limit(GridBarrier *bar, unsigned long 
     }
     __syncthreads();
     return s_ok != 0;
+}
+__device__ __forceinline__ bool grid_sync_limit(GridBarrier *bar, unsigned long long limit_ns) {
+    return grid_sync_nb(bar, gridDim.x * gridDim.y * gridDim.z, limit_ns);
 }
 __device__ __forceinline__ bool grid_sync(GridBarrier *bar) { return grid_sync_limit(bar, kBarrierTimeoutNs); }
 

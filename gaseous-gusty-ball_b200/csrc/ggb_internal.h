@@ -61,6 +61,19 @@ void stage_collect();  // after a stream sync: accumulate the recorded intervals
 void fluid_cfl_dt_launch(const Fluid *F, double cfl, double *dt_dev);
 void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks);
 void fluid_step_collect(Fluid *F);
+// The same step split around one batched solve launch (batch.cu): advection,
+// the solve's parameters (with the barrier the batched launch assigns), and
+// after the solve the result read-back and the velocity.
+struct SolveParams;
+void fluid_advect_queue(Fluid *F, const double *dt_dev);
+void fluid_step_solve_params(Fluid *F, GridBarrier *bar, SolveParams *out);
+int fluid_solve_mixed(const Fluid *F);
+double fluid_last_solve_seconds(const Fluid *F);
+void fluid_result_velocity_queue(Fluid *F);
+size_t pcg_launch_smem(const SolveParams &p);
+int pcg_batch_capacity(size_t smem, bool mixed);
+void pcg_launch_batch(const SolveParams *dev_prm, const int4 *dev_bmap, int nblocks, bool mixed, size_t smem,
+                      cudaStream_t s);
 void render_deposit_queue(Render *r, const Particles *P);
 void render_deposit_collect(Render *r, const Particles *P);
 void particles_advect_queue(Particles *P, const CubeSphere *cs, const float *vel, const double *dt_dev);

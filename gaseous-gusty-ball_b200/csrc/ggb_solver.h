@@ -40,6 +40,7 @@ struct SolveResult {
     double relres;
     int r_final;     // which r buffer holds the final residual (0: r, 1: r2)
     int flags;       // kSolve* bits
+    unsigned long long ns;  // device time of the solve (%globaltimer, block 0 of the solve)
 };
 
 struct SolveParams {

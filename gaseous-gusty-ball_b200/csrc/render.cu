@@ -34,13 +34,15 @@ constexpr int kT = 16;              // tile edge in texels
 constexpr int kMaxSamples = 4096;   // upstream cap on samples per arc
 
 // One splat sample on one tile: its compositing order key (particle index
-// << 13 | sample k), its texel-space centre on the tile's face and the
-// particle's colour (32 bytes: one DRAM sector).
+// << 13 | sample k) and its texel-space centre on the tile's face (16 bytes).
+// The particle's colour is not copied: compositing reads it from the
+// particles' colour array by the index in the key (an L2-resident gather),
+// which halves the record bytes that the fill writes and compositing reads.
 struct __align__(16) Rec {
     unsigned long long key;
     float px, py;
-    float4 col;
 };
+static_assert(sizeof(Rec) == 16, "a record is 16 bytes");
 
 struct SplatCfg {
     int R, ntx, ntiles;
@@ -275,8 +277,8 @@ __device__ __forceinline__ void append_rec(int tl, bool active, const Rec &r, co
 
 // Records of one (sample, face): one per tile its clamped footprint touches.
 __device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, float py, bool active,
-                                          unsigned long long key, float4 col, const unsigned *tile_start,
-                                          unsigned *tile_fill, Rec *recs, unsigned *diag) {
+                                          unsigned long long key, const unsigned *tile_start, unsigned *tile_fill,
+                                          Rec *recs, unsigned *diag) {
     Box bx = footprint(px, py, C.rad, C.R);
     if (bx.xlo > bx.xhi || bx.ylo > bx.yhi) active = false;
     const int tx0 = bx.xlo / kT, ty0 = bx.ylo / kT;
@@ -288,7 +290,6 @@ __device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, fl
     r.key = key;
     r.px = px;
     r.py = py;
-    r.col = col;
     for (int u = 0; u < most; u++) {
         const bool on = u < ntxs * ntys;
         // tile u of the footprint's ntxs x ntys tiles, row-major (a footprint
@@ -320,16 +321,14 @@ __device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, fl
 // edges only) follow.  Five blocks per SM (48 registers, a few bytes
 // spilled) ran 3 % faster than four.
 __global__ void __launch_bounds__(256, 5)
-    k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const float *col, const unsigned *tile_start,
-              unsigned *tile_fill, Rec *recs, size_t cap, unsigned *diag) {
+    k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const unsigned *tile_start, unsigned *tile_fill,
+              Rec *recs, size_t cap, unsigned *diag) {
     if (tile_start[C.ntiles] > cap) return;  // the host grows the record buffer and runs this again
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    const float4 *col4 = reinterpret_cast<const float4 *>(col);
     for (int base = warp * 32; base < n; base += nwarps * 32) {
         const int i = base + lane;
         float p0 = 0.f, p1 = 0.f, p2 = 0.f, q0 = 0.f, q1 = 0.f, q2 = 0.f;
-        float4 ci = make_float4(0.f, 0.f, 0.f, 0.f);
         int ns = 0;
         if (i < n) {
             p0 = prev[3 * (size_t)i];
@@ -338,7 +337,6 @@ __global__ void __launch_bounds__(256, 5)
             q0 = pos[3 * (size_t)i];
             q1 = pos[3 * (size_t)i + 1];
             q2 = pos[3 * (size_t)i + 2];
-            ci = col4[i];
             ns = arc_samples_f(p0, p1, p2, q0, q1, q2, C.spacing);
         }
         int incl = ns;
@@ -363,8 +361,6 @@ __global__ void __launch_bounds__(256, 5)
                             __shfl_sync(0xffffffffu, p2, j));
             const D3 b = d3(__shfl_sync(0xffffffffu, q0, j), __shfl_sync(0xffffffffu, q1, j),
                             __shfl_sync(0xffffffffu, q2, j));
-            const float4 cj = make_float4(__shfl_sync(0xffffffffu, ci.x, j), __shfl_sync(0xffffffffu, ci.y, j),
-                                          __shfl_sync(0xffffffffu, ci.z, j), __shfl_sync(0xffffffffu, ci.w, j));
             const bool live = t < total;
             const D3 d = arc_point(a, b, live ? k : 1, live ? nsj : 1);
             const unsigned long long key = ((unsigned long long)(base + j) << 13) | (unsigned)k;
@@ -374,7 +370,7 @@ __global__ void __launch_bounds__(256, 5)
                 const double u = dr / dc, v = du / dc;
                 const float px = (float)__fma_rn((u + 1.0) * 0.5, (double)C.R, -0.5);
                 const float py = (float)__fma_rn((1.0 - v) * 0.5, (double)C.R, -0.5);
-                emit_face(C, f0, px, py, live, key, cj, tile_start, tile_fill, recs, diag);
+                emit_face(C, f0, px, py, live, key, tile_start, tile_fill, recs, diag);
             }
             // other faces with d.c >= 0.5 (cube edges and corners)
             bool more = false;
@@ -389,7 +385,7 @@ __global__ void __launch_bounds__(256, 5)
                     float px = 0.f, py = 0.f;
                     const bool on = live && f != f0 && face_px(f, d, C.R, px, py);
                     if (__any_sync(0xffffffffu, on))
-                        emit_face(C, f, px, py, on, key, cj, tile_start, tile_fill, recs, diag);
+                        emit_face(C, f, px, py, on, key, tile_start, tile_fill, recs, diag);
                 }
             }
         }
@@ -588,12 +584,12 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
     return total;
 }
 
-// Record r with its box into slot s of the current window.
-__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box) {
+// Record r with its box and its particle's colour into slot s of the current window.
+__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box, const float4 *col) {
     S.u.r.key[s] = r.key;
     S.u.r.pos[s] = make_float2(r.px, r.py);
     S.box[s] = box;
-    S.col[s] = r.col;
+    S.col[s] = __ldg(col + (r.key >> 13));
 }
 
 // Blends the sorted entries e[0..m) of texel q into d (upstream
@@ -678,8 +674,8 @@ __device__ __forceinline__ void composite_window(TileSmem &S, int nw, const Spla
 // to that bucket.  One key is one record (a sample falls on a tile once), and
 // a record has at most 256 entries (its box lies on the tile), so every window
 // makes progress.
-__device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const SplatCfg &C, const TileGeo &G,
-                                   float4 &d) {
+__device__ void composite_windowed(TileSmem &S, const Rec *R, const float4 *col, int m, const SplatCfg &C,
+                                   const TileGeo &G, float4 &d) {
     const int tid = threadIdx.x, lane = tid & 31;
     unsigned long long kmin = ~0ull, kmax = 0;
     for (int s = tid; s < m; s += kTB) {
@@ -748,7 +744,7 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const Splat
             const unsigned short box = rec_box(C, G, r.px, r.py);
             if (box == kNoBox) continue;
             const int slot = atomicAdd(&S.cut, 1);
-            if (slot < kRec) window_put(S, slot, r, box);
+            if (slot < kRec) window_put(S, slot, r, box, col);
         }
         __syncthreads();
         const int nw = min(S.cut, kRec);
@@ -762,7 +758,7 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, int m, const Splat
 // registers left room for.
 __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned *tile_start,
                                                   const unsigned *tile_fill, const Rec *recs, size_t cap,
-                                                  float *buf, unsigned *diag) {
+                                                  const float4 *col, float *buf, unsigned *diag) {
     if (tile_start[C.ntiles] > cap) return;  // records not filled: see k_rd_fill
     if (diag[1]) return;                     // a tile's records overflowed: the deposit is repeated
     __shared__ TileSmem S;
@@ -806,7 +802,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
             for (int s = q; s < m; s += kTB) {
                 const Rec r = Rt[s];
                 const unsigned short box = rec_box(C, G, r.px, r.py);
-                window_put(S, s, r, box);
+                window_put(S, s, r, box, col);
                 box_texels(box, [&](int t) {
                     const int k = atomicAdd(&S.cnt[t], 1);
                     if (k < kBucket)
@@ -841,7 +837,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
         } else {
             if (q == 0) atomicAdd(diag, 1u);
             __syncthreads();
-            composite_windowed(S, Rt, m, C, G, d);
+            composite_windowed(S, Rt, col, m, C, G, d);
         }
     }
     if (inside) face[(size_t)(G.y0 + ly) * R + G.x0 + lx] = d;
@@ -887,11 +883,12 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
     const unsigned nb = (unsigned)std::max(1, std::min(n / 256 + 1, 148 * 16));
     stage_begin(ST_TILES);
     if (n > 0) {
-        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, P->col, Pv->tile_start, Pv->tile_fill, Pv->recs,
+        k_rd_fill<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_start, Pv->tile_fill, Pv->recs,
                                      Pv->rec_cap, Pv->diag);
         GGB_LAUNCHED();
     }
-    k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->rec_cap, r->buf, Pv->diag);
+    k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->rec_cap,
+                                          reinterpret_cast<const float4 *>(P->col), r->buf, Pv->diag);
     GGB_LAUNCHED();
     stage_end(ST_TILES);
 }

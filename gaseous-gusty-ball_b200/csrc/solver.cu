@@ -110,10 +110,17 @@ __device__ __forceinline__ typename Prec<MP>::A slot_w(const StencilDev &S, int 
     return __ldg(S.wslot_d + s * S.n + k);
 }
 
+// The block's place in its solve's grid (its "virtual grid"): the whole
+// launch for a single solve (blockIdx.x of gridDim.x), or the share of the
+// blocks of a batched launch that one planet's solve runs on.
+__shared__ int s_vgrid[2];
+__device__ __forceinline__ int vb() { return s_vgrid[0]; }
+__device__ __forceinline__ int vnb() { return s_vgrid[1]; }
+
 // Phase trace (diagnostics): block 0, thread 0 records (mark, %globaltimer).
 __device__ int g_trace_n;
 __device__ __forceinline__ void trace_mark(const SolveParams &P, int mark) {
-    if (P.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (P.trace && vb() == 0 && threadIdx.x == 0) {
         int k = g_trace_n;
         if (k < P.trace_cap) {
             P.trace[2 * k] = (unsigned long long)mark;
@@ -123,23 +130,32 @@ __device__ __forceinline__ void trace_mark(const SolveParams &P, int mark) {
     }
 }
 
-#define GRID_LOOP(c, n) for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < (n); c += gridDim.x * blockDim.x)
+#define GRID_LOOP(c, n) for (int c = vb() * blockDim.x + threadIdx.x; c < (n); c += vnb() * blockDim.x)
 #define BLOCK_LOOP(c, n) for (int c = threadIdx.x; c < (n); c += blockDim.x)
-#define SYNC_OR(fail)                    \
-    do {                                 \
-        if (!grid_sync(P.bar)) fail;     \
+#define SYNC_OR(fail)              \
+    do {                           \
+        if (!vsync(P)) fail;       \
     } while (0)
 
 struct Red {
     double v[kPB / 32 + 2];
 };
 
+// Barrier of the blocks of one solve (a block barrier when the solve has one block).
+__device__ __forceinline__ bool vsync(const SolveParams &P) {
+    if (vnb() == 1) {
+        __syncthreads();
+        return true;
+    }
+    return grid_sync_nb(P.bar, (unsigned)vnb(), kBarrierTimeoutNs);
+}
+
 __device__ __forceinline__ void put_partial(const SolveParams &P, int which, double v, double *s_red) {
     double t = block_sum<kPB>(v, s_red);
-    if (threadIdx.x == 0) P.part[which * gridDim.x + blockIdx.x] = t;
+    if (threadIdx.x == 0) P.part[which * vnb() + vb()] = t;
 }
 __device__ __forceinline__ double get_total(const SolveParams &P, int which, double *s_red) {
-    return sum_partials<kPB>(P.part + which * gridDim.x, gridDim.x, s_red);
+    return sum_partials<kPB>(P.part + which * vnb(), vnb(), s_red);
 }
 
 // ---- staged stencil phases ------------------------------------------------
@@ -152,7 +168,7 @@ __device__ __forceinline__ double get_total(const SolveParams &P, int which, dou
 // (or, at N = 512, another sub-range) and makes that block the phase's last.
 // Fewer blocks split the cells evenly.
 __device__ __forceinline__ void block_range(int n, int N, int &c0, int &c1) {
-    const int nb = gridDim.x, b = blockIdx.x;
+    const int nb = vnb(), b = vb();
     if (nb < 6) {
         c0 = (int)(((long long)n * b) / nb);
         c1 = (int)(((long long)n * (b + 1)) / nb);
@@ -637,7 +653,7 @@ __device__ bool vcycle_rest(const SolveParams &P, const float *r, float s0, floa
         const auto *cb = lv<MP>(C.b);
         auto *cx = lv<MP>(C.xo);
         const int nd = P.nd, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+        const int gw = vb() * (blockDim.x >> 5) + warp, nw = vnb() * (blockDim.x >> 5);
         for (int row = gw; row < nd; row += nw) {
             const double *d = P.dense + (size_t)row * nd;
             double acc = 0;
@@ -649,7 +665,7 @@ __device__ bool vcycle_rest(const SolveParams &P, const float *r, float s0, floa
         trace_mark(P, 500);
         SYNC_OR(return false);
     } else if (!P.coarse_on_grid) {
-        if (blockIdx.x == 0) {
+        if (vb() == 0) {
             SmemLevel lvs[kMaxLev];
             carve_smem(P, G, smem, lvs);
             const auto *gb = lv<MP>(P.L[G].b);
@@ -710,7 +726,7 @@ __device__ bool single_level(const SolveParams &P, const float *r, float s0, flo
     auto *lx = lv<MP>(L.x), *lxo = lv<MP>(L.xo);
     auto *lb = lv<MP>(L.b);
     if (!P.coarse_on_grid) {
-        if (blockIdx.x == 0) {
+        if (vb() == 0) {
             SmemLevel lvs[kMaxLev];
             carve_smem(P, 0, smem, lvs);
             BLOCK_LOOP(c, L.S.n) lvs[0].b[c] = r[c];
@@ -747,7 +763,7 @@ __device__ bool single_level(const SolveParams &P, const float *r, float s0, flo
     }
     put_partial(P, RED_RZ, s, s_red);
     if (MP) put_partial(P, RED_RZO, so, s_red);
-    return grid_sync(P.bar);
+    return vsync(P);
 }
 
 // Power of two that brings a residual of squared norm rr over n cells to an
@@ -759,8 +775,10 @@ __device__ __forceinline__ float vscale(double rr, int n) {
     return ldexpf(1.0f, max(-100, min(100, -4 - e)));
 }
 
+// The whole solve for the SolveParams of this block's planet, on the block's
+// virtual grid (vb(), vnb()).
 template <bool MP>
-__global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
+__device__ __forceinline__ void pcg_body(const SolveParams &P) {
     __shared__ Red sh;
     extern __shared__ __align__(16) unsigned char dyn[];
     double *buf = reinterpret_cast<double *>(dyn);               // staged window
@@ -778,6 +796,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     int it = 0, flags = 0;
     bool first = true, ok = true;
     float s0 = 1.0f;
+    const unsigned long long t_begin = threadIdx.x == 0 ? globaltimer_ns() : 0ull;
 
     // zero-mean projection of omega (FP64 sum), upstream src/fluid.c:264-275
     if (P.remove_mean) {
@@ -836,12 +855,13 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
     if (!isfinite(bb) || !isfinite(rr)) flags |= kSolveNonFinite;
     if (bb == 0.0) {
         GRID_LOOP(c, n) P.psi[c] = 0.f;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (vb() == 0 && threadIdx.x == 0) {
             P.res->iters = 0;
             P.res->relres = 0;
             P.res->status = 0;
             P.res->r_final = 0;
             P.res->flags = flags;
+            P.res->ns = globaltimer_ns() - t_begin;
         }
         return;
     }
@@ -865,7 +885,7 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
                 s += (double)r[c] * zc;
             }
             put_partial(P, RED_RZ, s, s_red);
-            ok = grid_sync(P.bar);
+            ok = vsync(P);
         }
         if (!ok) goto aborted;
         rz = get_total(P, RED_RZ, s_red);
@@ -1010,22 +1030,55 @@ __global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
         if (z != P.z) GRID_LOOP(c, n) P.z[c] = z[c];
     }
     if (it >= P.maxit && rr > tol2) flags |= kSolveMaxit;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (vb() == 0 && threadIdx.x == 0) {
         P.res->iters = it;
         P.res->relres = sqrt(rr / bb);
         P.res->status = 0;
         P.res->r_final = 0;
         P.res->flags = flags;
+        P.res->ns = globaltimer_ns() - t_begin;
     }
     return;
 
 aborted:
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (vb() == 0 && threadIdx.x == 0) {
         P.res->iters = it;
         P.res->relres = -1.0;
         P.res->status = 1;
         P.res->flags = flags | kSolveTimeout;
     }
+}
+
+// One solve on the whole grid.
+template <bool MP>
+__global__ void __launch_bounds__(kPB, 1) k_pcg(SolveParams P) {
+    if (threadIdx.x == 0) {
+        s_vgrid[0] = blockIdx.x;
+        s_vgrid[1] = gridDim.x;
+    }
+    __syncthreads();
+    pcg_body<MP>(P);
+}
+
+// Many planets' solves in one cooperative launch: block b runs planet
+// bmap[b].x's solve as block bmap[b].y of bmap[b].z (the planet's blocks are
+// consecutive), with that planet's parameters, barrier, partial sums and
+// result.  Planets finish independently.
+template <bool MP>
+__global__ void __launch_bounds__(kPB, 1) k_pcg_batch(const SolveParams *prm, const int4 *bmap) {
+    __shared__ SolveParams sP;
+    const int4 m = bmap[blockIdx.x];
+    {
+        const int *src = reinterpret_cast<const int *>(prm + m.x);
+        int *dst = reinterpret_cast<int *>(&sP);
+        for (int k = threadIdx.x; k < (int)(sizeof(SolveParams) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    }
+    if (threadIdx.x == 0) {
+        s_vgrid[0] = m.y;
+        s_vgrid[1] = m.z;
+    }
+    __syncthreads();
+    pcg_body<MP>(sP);
 }
 
 // ---- setup kernels -------------------------------------------------------
@@ -1160,6 +1213,39 @@ void pcg_launch(const SolveParams &prm, cudaStream_t s, int max_blocks) {
     if (max_blocks > 0) grid = std::max(1, std::min(grid, max_blocks));
     GGB_CHECK(cudaMemsetAsync(&p.bar->count, 0, sizeof(unsigned int), s));
     GGB_CHECK(cudaLaunchCooperativeKernel(pcg_kernel(p.mixed != 0), dim3(grid), dim3(kPB), args, smem, s));
+    GGB_LAUNCHED();
+}
+
+// Blocks of one batched solve launch that can be resident at once (the
+// launch's capacity), for the shared memory the planets' solves need.
+int pcg_batch_capacity(size_t smem, bool mixed) {
+    pcg_attributes();
+    const void *k = mixed ? (const void *)k_pcg_batch<true> : (const void *)k_pcg_batch<false>;
+    static bool attr[2] = {false, false};
+    if (!attr[mixed]) {
+        int dev = 0, optin = 0;
+        GGB_CHECK(cudaGetDevice(&dev));
+        GGB_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        GGB_CHECK(cudaFuncGetAttributes(&fa, k));
+        GGB_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+        attr[mixed] = true;
+    }
+    int per = 0;
+    GGB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kPB, smem));
+    return device_sm_count() * std::min(per, 2);
+}
+
+size_t pcg_launch_smem(const SolveParams &p) { return pcg_smem_bytes(p); }
+
+// One cooperative launch of nblocks blocks solving every planet of a batch
+// (dev_prm: the planets' parameters; dev_bmap: block -> planet, block of the
+// planet, blocks of the planet).  The planets' barrier counters must be zero.
+void pcg_launch_batch(const SolveParams *dev_prm, const int4 *dev_bmap, int nblocks, bool mixed, size_t smem,
+                      cudaStream_t s) {
+    const void *k = mixed ? (const void *)k_pcg_batch<true> : (const void *)k_pcg_batch<false>;
+    void *args[] = {(void *)&dev_prm, (void *)&dev_bmap};
+    GGB_CHECK(cudaLaunchCooperativeKernel(k, dim3(nblocks), dim3(kPB), args, smem, s));
     GGB_LAUNCHED();
 }
 

@@ -150,7 +150,10 @@ class Api:
             ("ggb_batch_create", C.c_void_p, [C.c_int, P(P(T["Fluid"])), P(P(T["Particles"])), P(P(T["Render"])),
                                               P(C.c_double), P(C.c_double)]),
             ("ggb_batch_step", C.c_int, [C.c_void_p, C.c_int]),
-            ("ggb_batch_cells_per_block", C.c_int, [C.c_void_p, C.c_int]),
+            ("ggb_batch_solve_blocks", C.c_int, [C.c_void_p, C.c_int]),
+            ("ggb_batch_blocks", None, [C.c_void_p, P(C.c_int)]),
+            ("ggb_batch_solve_ms", C.c_double, [C.c_void_p]),
+            ("ggb_batch_cost", C.c_double, [C.c_int, C.c_int]),
             ("ggb_batch_dt", None, [C.c_void_p, P(C.c_double)]),
             ("ggb_batch_free", None, [C.c_void_p]),
             ("ggb_batch_host_ms", C.c_double, [C.c_void_p, P(C.c_double), P(C.c_double)]),

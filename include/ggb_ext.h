@@ -151,24 +151,37 @@ int ggb_checkpoint_load(const char *path, Fluid *F, Particles *P, Render *r);
  * particles_init, render_init; planets of the same N may share a grid).
  * ggb_batch_step advances every planet by `steps` application-driver steps
  * (CFL dt from the maximum speed, particles_advect, fluid_step, render_fade,
- * render_deposit), queueing each planet's work on its own stream with the
- * CFL dt computed on the device, so that the planets' kernels overlap and
- * nothing returns to the host inside a step; it synchronises once per step.
- * A planet's solve runs on one block per `cells_per_block` cells (default
- * 2048, at most one per SM), so small planets solve side by side.  P[i] and
- * r[i] may be NULL (fluid only); fade[i] is render_fade's argument.
- * Results equal the per-planet entry points' up to the order of the solve's
- * FP64 block sums (a different grid) and the device's exp in the forcing's
- * relaxation factor.  create returns NULL with a message on bad arguments;
- * step returns 0. */
+ * render_deposit).  The Poisson solves of all planets run in one persistent
+ * cooperative launch, each planet on its own share of the blocks with its
+ * own barrier and convergence test; the shares come from an autotuner that
+ * estimates, from the solves' measured device times, a cost per cell for
+ * every grid size and precision, and equalises the planets' estimated
+ * finishing times (it refines the estimates over the first steps of a batch
+ * and keeps them for the process).  The other stages are queued on one
+ * stream per planet, the CFL dt is computed on the device, and the host
+ * synchronises once per step.  P[i] and r[i] may be NULL (fluid only);
+ * fade[i] is render_fade's argument.  Results equal the per-planet entry
+ * points' up to the order of the solve's FP64 block sums (another number of
+ * blocks) and the device's exp in the forcing's relaxation factor.  create
+ * returns NULL with a message on bad arguments; step returns 0. */
 typedef struct GGBBatch GGBBatch;
 GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *P, Render *const *r, const double *cfl,
                            const double *fade);
 int ggb_batch_step(GGBBatch *b, int steps);
-int ggb_batch_cells_per_block(GGBBatch *b, int cells); /* cells <= 0: query */
+/* blocks > 0: every planet's solve gets that many blocks (no tuning; at or
+ * above the launch's capacity, every planet is solved alone on all of it,
+ * which reproduces fluid_step's arithmetic exactly); 0: the autotuned shares
+ * (the default); < 0: query.  Returns the setting. */
+int ggb_batch_solve_blocks(GGBBatch *b, int blocks);
+void ggb_batch_blocks(const GGBBatch *b, int *blocks); /* each planet's blocks in the last step */
 void ggb_batch_dt(const GGBBatch *b, double *dt);      /* the last step's dt per planet */
 /* host time (ms) of the last step's queueing (returned), GPU wait and collection */
 double ggb_batch_host_ms(const GGBBatch *b, double *wait_ms, double *collect_ms);
+/* device time (ms) of the last step's batched solves (the slowest planet's) */
+double ggb_batch_solve_ms(const GGBBatch *b);
+/* the autotuner's estimate for grid N in the given precision: device seconds
+ * per cell for one block of a solve (0: not measured yet) */
+double ggb_batch_cost(int N, int mixed);
 void ggb_batch_free(GGBBatch *b);
 
 /* Initial-condition parameters of the application driver (bands and curl noise). */

@@ -573,9 +573,10 @@ def _batch_free(pls):
 @pytest.mark.parametrize("exact", [True, False])
 def test_batched_step_matches_per_planet(gpu, exact):
     """ggb_batch_step against the per-planet entry points (the driver's step
-    with dt = cfl h / vmax).  exact: one solve block per SM and no forcing,
-    so the batched arithmetic is the per-planet arithmetic, bit for bit;
-    otherwise small per-planet solve grids and forcing, within 1e-5."""
+    with dt = cfl h / vmax).  exact: every planet's solve alone on the whole
+    batched launch and no forcing, so the batched arithmetic is the
+    per-planet arithmetic, bit for bit; otherwise the planets share one
+    batched solve launch (autotuned shares) and forcing is on, within 1e-5."""
     specs = [(16, 1500, 32, 3), (32, 3000, 40, 4), (24, 2000, 32, 5)]
     forcing, rotation = (0.0, 2.0) if exact else (0.5, 2.0)
     steps, cfl, fade = 3, 1.0, 0.02
@@ -601,7 +602,7 @@ def test_batched_step_matches_per_planet(gpu, exact):
     b = gpu.lib.ggb_batch_create(n, Fs, Ps, Rs, cf, fd)
     assert b
     if exact:
-        gpu.lib.ggb_batch_cells_per_block(b, 1)
+        gpu.lib.ggb_batch_solve_blocks(b, 1 << 20)
     assert gpu.lib.ggb_batch_step(b, steps) == 0
     got = [_batch_state(pl) for pl in bat]
     gpu.lib.ggb_batch_free(b)
@@ -640,7 +641,7 @@ def test_batched_step_fluid_only_planet(gpu):
     fd = (C.c_double * 2)(0.02, 0.0)
     b = gpu.lib.ggb_batch_create(2, Fs, Ps, Rs, cf, fd)
     assert b
-    gpu.lib.ggb_batch_cells_per_block(b, 1)
+    gpu.lib.ggb_batch_solve_blocks(b, 1 << 20)
     assert gpu.lib.ggb_batch_step(b, steps) == 0
     got = (fs.field("omega").copy(), fs.field("psi").copy(), fs.field("vel", 3).copy())
     gpu.lib.ggb_batch_free(b)
