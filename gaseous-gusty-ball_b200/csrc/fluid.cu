@@ -149,24 +149,40 @@ __global__ void k_cfl_dt(const unsigned int *vmax_bits, double cfl, double h, do
 
 // ------------------------------------------------------------ advection
 
-// Midpoint backtraces (backward and, for BFECC, forward) and q0 = omega + 2 Omega y.
-// upstream src/fluid.c:397-414, 435-437
+// Absolute vorticity q0 = omega + 2 Omega y of cell j, as FP32 (upstream
+// src/fluid.c:435-437).
+__device__ __forceinline__ float q0_of(const float *omega, const float *pos, double two_omega, int j) {
+    return (float)(__ldg(omega + j) + two_omega * __ldg(pos + 3 * j + 1));
+}
+
+// Midpoint backtraces (backward and, for BFECC, forward), q0 = omega + 2 Omega y
+// and the first resample q1 = q0 at the backward departure point, in one pass
+// (upstream src/fluid.c:397-414, 435-441).  q0 at the four taps is formed from
+// omega and the positions instead of being read back from q0, which this
+// kernel is writing; the sample point is the departure point as stored
+// (FP32), so q1 equals a separate resample of the stored q0 bit for bit.
 // dt: the time step, or *dtp when dtp is not null (a device-side CFL step).
 __global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt_in,
                              const double *dtp, double two_omega, int forward, float *dep_b, float *dep_f,
-                             float *q0) {
+                             float *q0, float *q1) {
     const double dt = dtp ? *dtp : dt_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
         D3 p = load3(pos + 3 * i), u = load3(vel + 3 * i);
         D3 pm = sphere_move(p, u, -0.5 * dt);
         D3 um = tangent(sample_vec(g, vel, pm), p);
-        store3(dep_b + 3 * i, sphere_move(p, um, -dt));
+        float *db = dep_b + 3 * i;
+        store3(db, sphere_move(p, um, -dt));
         if (forward) {
             pm = sphere_move(p, u, 0.5 * dt);
             um = tangent(sample_vec(g, vel, pm), p);
             store3(dep_f + 3 * i, sphere_move(p, um, dt));
         }
-        q0[i] = (float)(omega[i] + two_omega * pos[3 * i + 1]);
+        q0[i] = q0_of(omega, pos, two_omega, i);
+        int idx[4];
+        double wt[4];
+        taps(g, load3(db), idx, wt);
+        q1[i] = (float)(wt[0] * q0_of(omega, pos, two_omega, idx[0]) + wt[1] * q0_of(omega, pos, two_omega, idx[1]) +
+                        wt[2] * q0_of(omega, pos, two_omega, idx[2]) + wt[3] * q0_of(omega, pos, two_omega, idx[3]));
     }
 }
 
@@ -753,9 +769,7 @@ static void advect_launch(Fluid *F, FluidPriv *Pv, double dt, const double *dtp)
     unsigned nb = blocks_for(t->n);
     stage_begin(ST_ADVECT);
     k_departures<<<nb, kB, 0, s>>>(g, t->pos, F->vel, F->omega, dt, dtp, two_omega, bfecc, F->dep_b, F->dep_f,
-                                   F->q0);
-    GGB_LAUNCHED();
-    k_resample<<<nb, kB, 0, s>>>(g, F->q0, F->dep_b, F->q0, 0, F->q1);
+                                   F->q0, F->q1);
     GGB_LAUNCHED();
     if (bfecc) {
         k_resample<<<nb, kB, 0, s>>>(g, F->q1, F->dep_f, F->q0, 1, F->q2);

@@ -100,14 +100,15 @@ __device__ __forceinline__ float prolong_scale() {
     return MP ? 4.0f : 1.0f;
 }
 
-// Slot weight s of cell k, as the stencil's accumulation type.
+// Slot weight at index q (= s * n + cell) of a level's FP64 (plain), FP16
+// (mixed, when present) or FP32 slot table, as the stencil's accumulation type.
 template <bool MP>
-__device__ __forceinline__ typename Prec<MP>::A slot_w(const StencilDev &S, int s, int k) {
+__device__ __forceinline__ typename Prec<MP>::A slot_w(const double *wd, const float *wf, const __half *wh, int q) {
     if (MP) {
-        if (S.wslot_h) return __half2float(S.wslot_h[s * S.n + k]);
-        return __ldg(S.wslot + s * S.n + k);
+        if (wh) return __half2float(wh[q]);
+        return __ldg(wf + q);
     }
-    return __ldg(S.wslot_d + s * S.n + k);
+    return __ldg(wd + q);
 }
 
 // The block's place in its solve's grid (its "virtual grid"): the whole
@@ -130,7 +131,10 @@ __device__ __forceinline__ void trace_mark(const SolveParams &P, int mark) {
     }
 }
 
+// GRID_LOOP: over the block's virtual grid (only inside k_pcg / k_pcg_batch,
+// which set it); KERNEL_LOOP: over the launch's real grid (set-up kernels).
 #define GRID_LOOP(c, n) for (int c = vb() * blockDim.x + threadIdx.x; c < (n); c += vnb() * blockDim.x)
+#define KERNEL_LOOP(c, n) for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < (n); c += gridDim.x * blockDim.x)
 #define BLOCK_LOOP(c, n) for (int c = threadIdx.x; c < (n); c += blockDim.x)
 #define SYNC_OR(fail)              \
     do {                           \
@@ -233,6 +237,10 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *raw, Load lo
     A *bx = buf, *b0 = buf + kStageCap, *b1 = buf + 2 * kStageCap, *b2 = buf + 3 * kStageCap, *b3 = buf + 4 * kStageCap;
     float *oa = reinterpret_cast<float *>(buf + 5 * kStageCap), *ob = oa + kStageCap, *oc = ob + kStageCap;
     A *rs = reinterpret_cast<A *>(oc + kStageCap);
+    // the slot tables, read once into registers (not per window cell)
+    const double *wd = S.wslot_d;
+    const float *wf = S.wslot;
+    const __half *wh = S.wslot_h;
     stage_mark(1);
     for (int s0 = c0; s0 < c1;) {
         int s1 = min(c1, s0 + sub);
@@ -275,18 +283,18 @@ __device__ __forceinline__ void staged(const StencilDev &S, double *raw, Load lo
             Own o1{0.f, 0.f, 0.f, 0.f}, o2{0.f, 0.f, 0.f, 0.f};
             A e1 = 0, n1 = 0, ne1 = 0, nw1 = 0, v1 = 0;
             if (k >= 0 && k < n) {
-                e1 = slot_w<MP>(S, 0, k);
-                n1 = slot_w<MP>(S, 1, k);
-                ne1 = slot_w<MP>(S, 2, k);
-                nw1 = slot_w<MP>(S, 3, k);
+                e1 = slot_w<MP>(wd, wf, wh, k);
+                n1 = slot_w<MP>(wd, wf, wh, n + k);
+                ne1 = slot_w<MP>(wd, wf, wh, 2 * n + k);
+                nw1 = slot_w<MP>(wd, wf, wh, 3 * n + k);
                 v1 = load(k, in1, o1);
             }
             A e2 = 0, n2 = 0, ne2 = 0, nw2 = 0, v2 = 0;
             if (two && k2 >= 0 && k2 < n) {
-                e2 = slot_w<MP>(S, 0, k2);
-                n2 = slot_w<MP>(S, 1, k2);
-                ne2 = slot_w<MP>(S, 2, k2);
-                nw2 = slot_w<MP>(S, 3, k2);
+                e2 = slot_w<MP>(wd, wf, wh, k2);
+                n2 = slot_w<MP>(wd, wf, wh, n + k2);
+                ne2 = slot_w<MP>(wd, wf, wh, 2 * n + k2);
+                nw2 = slot_w<MP>(wd, wf, wh, 3 * n + k2);
                 v2 = load(k2, in2, o2);
             }
             if (in1) commit(k, o1);
@@ -1105,7 +1113,7 @@ __global__ void __launch_bounds__(kPB, 1) k_dense_columns(SolveParams P, int l0,
 // row (which the structured check has verified to be that window in order).
 __global__ void k_build_rw16(LevelDev F, LevelDev C, float *rw16) {
     const int Nc = C.S.N, nc = C.S.n;
-    GRID_LOOP(c, nc) {
+    KERNEL_LOOP(c, nc) {
         int f, I, J;
         cell_fij(C.S, c, f, I, J);
         const bool inner = I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc;
@@ -1118,7 +1126,7 @@ __global__ void k_build_rw16(LevelDev F, LevelDev C, float *rw16) {
 // take but that do not follow the structured index pattern.
 __global__ void k_check_structured(LevelDev F, LevelDev C, int *bad) {
     const int Nf = F.S.N, Nc = C.S.N;
-    GRID_LOOP(c, C.S.n) {
+    KERNEL_LOOP(c, C.S.n) {
         int f, I, J;
         cell_fij(C.S, c, f, I, J);
         if (!(I >= 1 && J >= 1 && I + 2 <= Nc && J + 2 <= Nc)) continue;
@@ -1135,7 +1143,7 @@ __global__ void k_check_structured(LevelDev F, LevelDev C, int *bad) {
                 if (F.ridx[q] != i || F.rw[q] != F.pw[4 * i + k]) atomicAdd(bad, 1);
             }
     }
-    GRID_LOOP(i, F.S.n) {
+    KERNEL_LOOP(i, F.S.n) {
         int f, fi, fj;
         cell_fij(F.S, i, f, fi, fj);
         const int I0 = (fi - 1) >> 1, J0 = (fj - 1) >> 1;

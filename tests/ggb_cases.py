@@ -87,9 +87,36 @@ def operators(api, N):
     return dict(lap=y, curl=curl, div=div, mean_removed=f)
 
 
-def poisson(api, N, tol=1e-6, maxit=5000, mixed=False):
+TABLE_KEYS = ("pos", "area", "nnb", "nbr", "w", "elen", "gc")
+
+
+def tables_of(api, N):
+    """The public grid tables of `api`'s cs_init(N) (copies) and its total area."""
+    g = api.grid(N)
+    out = {k: v.copy() for k, v in g.arrays().items()}
+    out["total_area"] = float(g.cs.total_area)
+    g.free()
+    return out
+
+
+def load_tables(api, g, tables):
+    """Overwrites the public tables of grid g (before any fluid_init on it)
+    with `tables`, so that a library built with FP64 storage solves exactly
+    the discrete problem whose FP32 tables another library built: its
+    operators read these arrays.  (The upstream FP32 and FP64 builds compute
+    different grids: the FP64 build keeps cell positions in double, and its
+    cell areas differ from the FP32 build's by up to 0.2 %.)"""
+    a = g.arrays()
+    for k in TABLE_KEYS:
+        a[k][...] = tables[k].astype(a[k].dtype)
+    g.cs.total_area = tables["total_area"]
+
+
+def poisson(api, N, tol=1e-6, maxit=5000, mixed=False, tables=None):
     """upstream tests/test_poisson.c:51-72: solve Laplacian(psi) = lap_exact."""
     g = api.grid(N)
+    if tables is not None:
+        load_tables(api, g, tables)
     fs = G.FluidSim(api, g, cg_tol=tol, cg_maxit=maxit, mixed=mixed)
     pos = g.arrays()["pos"].astype(np.float64)
     om = fs.field("omega")
@@ -117,12 +144,15 @@ def initial_velocity(api, g, seed=1, bands=8):
 
 
 def run(api, N, particles, R, steps, vel0, vband, forcing=0.5, rotation=3.0, tol=1e-6, fixed_dt=0.0,
-        cfl=1.0, fade=0.02, strip_seed=1, bfecc=1, snaps=(), dts_in=None, maxit=500, mixed=False):
+        cfl=1.0, fade=0.02, strip_seed=1, bfecc=1, snaps=(), dts_in=None, maxit=500, mixed=False, tables=None):
     """The application driver's step loop (upstream src/main.c:421-438):
     dt from CFL, particles_advect, fluid_step, render_fade, render_deposit.
     snaps: steps after which the state is recorded in out["snap"][step];
-    dts_in: the time step of every step (instead of the CFL step)."""
+    dts_in: the time step of every step (instead of the CFL step);
+    tables: grid tables to load into the grid first (load_tables)."""
     g = api.grid(N)
+    if tables is not None:
+        load_tables(api, g, tables)
     fs = G.FluidSim(api, g, forcing=forcing, rotation=rotation, cg_tol=tol, bfecc=bfecc, cg_maxit=maxit, mixed=mixed)
     nr = api.np_real
     fs.set_state(np.asarray(vel0, nr), None if vband is None else np.asarray(vband, nr))
@@ -197,3 +227,19 @@ def random_arcs(n, seed, max_angle):
     b = a * np.cos(th) + t * np.sin(th)
     col = rng.uniform(0.05, 1.0, size=(n, 4))
     return a.astype(np.float32), b.astype(np.float32), col.astype(np.float32)
+
+
+def solve_fp64(orc64, N, tables, omega, tol=1e-12):
+    """psi and u of the FP64 oracle solving omega on the given grid tables
+    (remove_mean, fluid_solve_psi, fluid_compute_velocity)."""
+    g = orc64.grid(N)
+    load_tables(orc64, g, tables)
+    fs = G.FluidSim(orc64, g, cg_tol=tol, cg_maxit=20000)
+    fs.field("omega")[:] = np.asarray(omega, np.float64)
+    orc64.lib.fluid_remove_mean(C.byref(g.cs), fs.F.omega)
+    orc64.lib.fluid_solve_psi(C.byref(fs.F))
+    orc64.lib.fluid_compute_velocity(C.byref(fs.F))
+    out = dict(psi=fs.field("psi").copy(), vel=fs.field("vel", 3).copy())
+    fs.free()
+    g.free()
+    return out

@@ -208,15 +208,23 @@ def test_run_golden(gpu):
 
 def test_fp32_path_error_vs_fp64_oracle(gpu, orc64):
     """psi / u / particle error of the FP32 GPU path against the FP64 oracle
-    (tol 1e-10) after 10 steps of fixed dt on N=32."""
+    (tol 1e-10) on the same grid tables, after 10 steps of fixed dt on N=32
+    (the FP64 build's own grid differs by up to 0.2 % in cell area, which is
+    not a precision error; ggb_cases.load_tables)."""
     g = orc64.grid(32)
     v64, b64 = K.initial_velocity(orc64, g, seed=2)
     g.free()
+    tab = K.tables_of(gpu, 32)
     h = (np.pi / 2) / 32
     a = K.run(gpu, 32, 2000, 64, 10, v64.astype(np.float32), b64.astype(np.float32), tol=1e-6, fixed_dt=h / 2)
-    b = K.run(orc64, 32, 2000, 64, 10, v64, b64, tol=1e-10, fixed_dt=h / 2)
-    assert rel_l2(a["psi"], b["psi"]) < 1e-4
-    assert rel_l2(a["vel"], b["vel"]) < 1e-4
+    b = K.run(orc64, 32, 2000, 64, 10, v64, b64, tol=1e-10, fixed_dt=h / 2, tables=tab)
+    e = {k: rel_l2(a[k], b[k]) for k in ("psi", "vel", "omega")}
+    ang = np.arccos(np.clip(np.sum(a["pos"] * b["pos"], 1) / np.linalg.norm(a["pos"], axis=1)
+                            / np.linalg.norm(b["pos"], axis=1), -1, 1))
+    print(f"FP32 path vs FP64 oracle, N=32, 10 steps: {e}, particle angle max {ang.max():.2e}")
+    assert e["psi"] <= 1e-5 and e["omega"] <= 1e-5
+    assert e["vel"] <= 5e-5
+    assert ang.max() < 1e-5
 
 
 # ---------------------------------------------------------------- render
