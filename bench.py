@@ -55,9 +55,10 @@ def args_():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["default", "large", "batch"], default="default",
+    p.add_argument("--workload", choices=["default", "large", "batch", "batch-large"], default="default",
                    help="large: N=512, 4M particles, 2048^2 faces, forcing 0.5, rotation 10; "
-                        "batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping")
+                        "batch: 64 uneven planets (N in {64,128,256}), batched step against per-planet stepping; "
+                        "batch-large: 16 x N=512 planets + one N=1024 planet with 16M particles and 4096^2 faces")
     p.add_argument("--precision", choices=["plain", "mixed"], default=None,
                    help="plain: FP32 solve with FP64 stencil sums; mixed: FP16 V-cycle storage, FP32 accumulation, "
                         "flexible CG (FP64 dots and mean projections in both).  Default: plain, except mixed for "
@@ -211,8 +212,7 @@ def fp64_error(ref_pl, dts, cfg, mixed):
     rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
     p_g = gp.ps.array("pos", 3).astype(np.float64)
     p_r = ref_pl.ps.array("pos", 3)
-    cosang = np.sum(p_g * p_r, 1) / np.linalg.norm(p_g, axis=1) / np.linalg.norm(p_r, axis=1)
-    ang = np.arccos(np.clip(cosang, -1, 1))
+    ang = np.arctan2(np.linalg.norm(np.cross(p_g, p_r), axis=1), np.sum(p_g * p_r, 1))
     out = {"steps": len(dts), "psi_rel_l2": rel(gp.fs.field("psi"), f64.field("psi")),
            "u_rel_l2": rel(gp.fs.field("vel", 3), f64.field("vel", 3)),
            "omega_rel_l2": rel(gp.fs.field("omega"), f64.field("omega")),
@@ -719,6 +719,134 @@ def run_batch(a, rank, world, local):
         dist.destroy_process_group()
 
 
+def large_batch_specs(seed=9):
+    """16 planets at N=512 with 1M particles and 1024^2 faces each, plus one
+    planet at N=1024 with 16M particles and 4096^2 faces; forcing 1.0 toward
+    band vorticity, rotation 20; one seed per planet."""
+    out = [dict(CFG, N=512, particles=1_000_000, R=1024, forcing=1.0, rotation=20.0, seed=seed * 1000 + i)
+           for i in range(16)]
+    out.append(dict(CFG, N=1024, particles=16_000_000, R=4096, forcing=1.0, rotation=20.0, seed=seed * 1000 + 16))
+    return out
+
+
+def _make_planets(api, specs, mixed):
+    grids, planets = {}, []
+    for sp in specs:
+        if sp["N"] not in grids:
+            grids[sp["N"]] = api.grid(sp["N"])
+        g = grids[sp["N"]]
+        ip = G.InitParams(sp["bands"], sp["band_amp"], sp["noise_amp"], sp["noise_scale"], sp["noise_lacunarity"],
+                          sp["noise_gain"], sp["noise_octaves"], sp["seed"])
+        vel = np.zeros(3 * g.n, api.np_real)
+        vb = np.zeros(3 * g.n, api.np_real)
+        api.lib.ggb_initial_velocity(C.byref(g.cs), C.byref(ip), api.ptr(vel), api.ptr(vb))
+        fs = G.FluidSim(api, g, forcing=sp["forcing"], rotation=sp["rotation"], cg_tol=sp["cg_tol"],
+                        cg_maxit=sp["cg_maxit"], mixed=mixed)
+        fs.set_state(vel, vb if sp["forcing"] > 0 else None)
+        ps = G.ParticleSet(api, sp["particles"])
+        ps.colour(ggb_inputs.strip(sp["seed"]))
+        spl = G.Splat(api, sp["R"], sp["radius"], sp["alpha"])
+        planets.append((g, fs, ps, spl, sp))
+    return grids, planets
+
+
+def _free_planets(grids, planets):
+    for g, fs, ps, spl, sp in planets:
+        spl.free()
+        ps.free()
+        fs.free()
+    for g in grids.values():
+        g.free()
+
+
+def run_batch_large(a, rank, world, local):
+    """16 x N=512 planets plus one N=1024 planet (16M particles, 4096^2
+    faces), batched with the mixed-precision solve, against the same planets
+    from the same initial states stepped through the per-planet entry points
+    with the plain FP32 solve; the face images of the two are compared."""
+    api = G.Api(G.PRODUCT_LIB)
+    if api.lib.ggb_set_device(local) != 0:
+        raise RuntimeError(f"cannot select CUDA device {local}")
+    for name, res, args in (("ggb_timer_start", None, []), ("ggb_timer_stop", C.c_double, [])):
+        fn = getattr(api.lib, name)
+        fn.restype, fn.argtypes = res, args
+    specs = large_batch_specs()
+    ga, pa = _make_planets(api, specs, mixed=True)
+    gb, pb = _make_planets(api, specs, mixed=False)
+    n = len(pa)
+    T = api.T
+    Fs = (C.POINTER(T["Fluid"]) * n)(*[C.pointer(p[1].F) for p in pa])
+    Ps = (C.POINTER(T["Particles"]) * n)(*[C.pointer(p[2].P) for p in pa])
+    Rs = (C.POINTER(T["Render"]) * n)(*[C.pointer(p[3].r) for p in pa])
+    cf = (C.c_double * n)(*[p[4]["cfl"] for p in pa])
+    fd = (C.c_double * n)(*[p[4]["fade"] for p in pa])
+    b = api.lib.ggb_batch_create(n, Fs, Ps, Rs, cf, fd)
+    K = max(2, min(a.steps, 10))
+
+    def plain_step(p):
+        g, fs, ps, spl, sp = p
+        lib = api.lib
+        vmax = lib.fluid_max_speed(C.byref(fs.F))
+        dt = sp["cfl"] * g.cs.h / (vmax if vmax > 1e-6 else 1e-6)
+        lib.particles_advect(C.byref(ps.P), C.byref(g.cs), fs.F.vel, dt)
+        lib.fluid_step(C.byref(fs.F), dt)
+        lib.render_fade(C.byref(spl.r), sp["fade"])
+        lib.render_deposit(C.byref(spl.r), C.byref(ps.P))
+
+    clk, clk_path = start_clock_sampler(local)
+    time.sleep(0.3)
+    api.lib.ggb_timer_start()
+    t0 = time.perf_counter()
+    api.lib.ggb_batch_step(b, K)
+    ms_b = max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0))
+    api.lib.ggb_timer_start()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        for p in pb:
+            plain_step(p)
+    ms_p = max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0))
+    clocks = stop_clock_sampler(clk, clk_path)
+    its = [p[1].F.cg_iters for p in pa]
+    blocks = (C.c_int * n)()
+    api.lib.ggb_batch_blocks(b, blocks)
+    # faces of the batched (mixed) and the plain planets, as the driver's 8-bit images
+    cmp = []
+    for p, q in zip(pa, pb):
+        R = p[4]["R"]
+        ia = np.zeros(6 * R * R * 4, np.uint8)
+        ib = np.zeros(6 * R * R * 4, np.uint8)
+        api.lib.ggb_encode_faces(C.byref(p[3].r), None, None, ia.ctypes.data_as(C.POINTER(C.c_ubyte)))
+        api.lib.ggb_encode_faces(C.byref(q[3].r), None, None, ib.ctypes.data_as(C.POINTER(C.c_ubyte)))
+        d = np.abs(ia.astype(np.int16) - ib.astype(np.int16))
+        psi_a, psi_b = p[1].field("psi").astype(np.float64), q[1].field("psi").astype(np.float64)
+        cmp.append({"N": p[4]["N"], "R": R, "face_levels_max": int(d.max()),
+                    "face_frac_over_1_level": float((d > 1).mean()), "face_mean_abs_levels": float(d.mean()),
+                    "psi_rel_l2_vs_plain": float(np.linalg.norm(psi_a - psi_b) / np.linalg.norm(psi_b))})
+    api.lib.ggb_batch_free(b)
+    value = n * K / (ms_b / 1000.0)
+    plain = n * K / (ms_p / 1000.0)
+    worst = max(cmp, key=lambda c: c["face_frac_over_1_level"])
+    print(json.dumps({
+        "metric": "planet-steps/s (16 x N=512 + 1 x N=1024 planets, batched)", "value": value,
+        "unit": "planet-steps/s", "n_gpus": world, "steps": K, "warmup": 0, "ms_per_step": ms_b / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f16", "data": "synthetic",
+        "plain": {"value": plain, "unit": "planet-steps/s", "ms_per_step": ms_p / K,
+                  "note": "the same planets from the same initial states, per-planet entry points, plain FP32"},
+        "speedup_vs_plain": value / plain,
+        "config": {"workload": "16 planets at N=512 (1M particles, 1024^2 faces) + 1 planet at N=1024 (16M "
+                               "particles, 4096^2 faces), forcing 1.0, rotation 20, PCG tol 1e-6, CFL 1; "
+                               f"{K} steps from the initial state (the workload's 1000 steps are not timed)",
+                   "precision": "batched: mixed (FP16 V-cycle, flexible CG); plain: FP32",
+                   "mean_cg_iters": float(np.mean(its)), "solve_blocks": [int(x) for x in blocks],
+                   "face_comparison": {"worst_planet": worst, "planets": cmp,
+                                       "tolerance": "8-bit face images (render_pixel8 of every texel) of the "
+                                                    "batched mixed-precision run against the plain per-planet "
+                                                    "run after the same steps"}},
+        "clocks": clocks}), flush=True)
+    _free_planets(ga, pa)
+    _free_planets(gb, pb)
+
+
 def main():
     a = args_()
     rank = int(os.environ.get("RANK", 0))
@@ -735,6 +863,8 @@ def main():
         run_reference(a, rank, world)
     elif a.workload == "batch":
         run_batch(a, rank, world, local)
+    elif a.workload == "batch-large":
+        run_batch_large(a, rank, world, local)
     else:
         run_ours(a, rank, world, local)
 

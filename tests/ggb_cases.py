@@ -243,3 +243,13 @@ def solve_fp64(orc64, N, tables, omega, tol=1e-12):
     fs.free()
     g.free()
     return out
+
+
+def angle_between(a, b):
+    """Angle (rad) between corresponding rows of two arrays of 3-vectors, in
+    FP64 as atan2(|a x b|, a . b): accurate for small angles, where the
+    arccos of a normalised dot product loses half the digits (FP32 norms of
+    unit vectors alone would read as angles of some 1e-4)."""
+    a = np.asarray(a, np.float64).reshape(-1, 3)
+    b = np.asarray(b, np.float64).reshape(-1, 3)
+    return np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.sum(a * b, 1))

@@ -34,9 +34,7 @@ def rel_l2(a, b):
 
 
 def angles(a, b):
-    a, b = np.asarray(a, np.float64).reshape(-1, 3), np.asarray(b, np.float64).reshape(-1, 3)
-    c = np.sum(a * b, 1) / np.linalg.norm(a, axis=1) / np.linalg.norm(b, axis=1)
-    return np.arccos(np.clip(c, -1.0, 1.0))
+    return K.angle_between(a, b)
 
 
 def compare(a, b):

@@ -190,8 +190,7 @@ def test_short_run(gpu, orc32, bfecc):
     assert np.max(np.abs(a["dts"] - b["dts"]) / b["dts"]) < 1e-5
     for k in ("omega0", "psi0", "vel0", "omega", "psi", "vel"):
         assert rel_l2(a[k], b[k]) < 1e-4, (k, rel_l2(a[k], b[k]))
-    ang = np.arccos(np.clip(np.sum(a["pos"] * b["pos"], 1) / np.linalg.norm(a["pos"], axis=1)
-                            / np.linalg.norm(b["pos"], axis=1), -1, 1))
+    ang = K.angle_between(a["pos"], b["pos"])
     assert np.median(ang) < 1e-6 and np.percentile(ang, 99) < 1e-5
     assert np.max(np.abs(a["faces"] - b["faces"])) < 1e-3
     assert np.mean(np.abs(a["faces"] - b["faces"])) < 1e-6
@@ -219,12 +218,10 @@ def test_fp32_path_error_vs_fp64_oracle(gpu, orc64):
     a = K.run(gpu, 32, 2000, 64, 10, v64.astype(np.float32), b64.astype(np.float32), tol=1e-6, fixed_dt=h / 2)
     b = K.run(orc64, 32, 2000, 64, 10, v64, b64, tol=1e-10, fixed_dt=h / 2, tables=tab)
     e = {k: rel_l2(a[k], b[k]) for k in ("psi", "vel", "omega")}
-    ang = np.arccos(np.clip(np.sum(a["pos"] * b["pos"], 1) / np.linalg.norm(a["pos"], axis=1)
-                            / np.linalg.norm(b["pos"], axis=1), -1, 1))
+    ang = K.angle_between(a["pos"], b["pos"])
     print(f"FP32 path vs FP64 oracle, N=32, 10 steps: {e}, particle angle median {np.median(ang):.2e}, "
           f"p99 {np.percentile(ang, 99):.2e}, max {ang.max():.2e}")
-    # measured: psi 7.9e-7, u 4.2e-7, omega 7.3e-7; the angle's maximum (2.6e-4, one particle
-    # of 2000 whose taps change cell) is reported, the median and 99th percentile are bounded
+    # measured: psi 7.9e-7, u 4.2e-7, omega 7.3e-7
     assert e["psi"] <= 1e-5 and e["omega"] <= 1e-5
     assert e["vel"] <= 5e-5
     assert np.median(ang) < 1e-6 and np.percentile(ang, 99) < 1e-5
