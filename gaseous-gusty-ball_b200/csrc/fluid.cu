@@ -334,6 +334,7 @@ struct FluidPriv {
     double *dense = nullptr;       // dense map of the V-cycle below the grid levels
     int nd = 0;
     int last_flags = 0;            // kSolve* bits of the last solve
+    int fuse_from = 2;             // SolveParams::fuse_from of this fluid's solves
     // mixed-precision solve (ggb_fluid_set_precision): FP16 level vectors,
     // FP16 slot weights of the coarse levels, the previous z
     int mixed = 0;
@@ -425,6 +426,7 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
     const bool mg = F->prm.multigrid != 0;
     P.nlev = mg ? Pv->nlev : 0;
     P.coarse_sweeps = 60;
+    P.fuse_from = Pv->fuse_from;
     P.remove_mean = remove_mean;
     P.maxit = maxit;
     P.tol = F->prm.cg_tol;
@@ -676,6 +678,16 @@ GGB_EXPORT void fluid_free(Fluid *F) {
     cudaFreeHost(Pv->vmax_host);
     delete Pv;
     memset(F, 0, sizeof(*F));
+}
+
+// The first multigrid level whose restriction is formed inside its pre-smooth
+// phase (see SolveParams::fuse_from); 0 turns the fusion off.  Returns the
+// previous value; a negative level only queries.
+GGB_EXPORT int ggb_fluid_fuse_from(Fluid *F, int level) {
+    FluidPriv *Pv = priv_of(F);
+    const int old = Pv->fuse_from;
+    if (level >= 0) Pv->fuse_from = level;
+    return old;
 }
 
 // Status bits of the last solve of F (kSolve* in ggb_solver.h; see ggb_ext.h).
