@@ -18,9 +18,13 @@
 //     time is minimised under the launch's capacity).  The estimates are kept
 //     per grid size for the life of the process, so a later batch with the
 //     same grid sizes starts from them;
-//   - the work before and after the solve (CFL dt, particle advection, the
-//     BFECC advection; velocity, fade and splat) is queued on one stream per
-//     planet, so the kernels of different planets overlap;
+//   - the per-cell and per-particle stages around the solve (maximum speed
+//     and CFL dt, particle advection, departures + BFECC + limiter, velocity)
+//     are one launch per stage for all planets: each block finds its planet
+//     and its share of that planet's cells or particles in a block map, with
+//     the per-planet kernels' arithmetic;
+//   - fade and splat are queued on one stream per planet after the velocity,
+//     so the deposits of different planets overlap;
 //   - the CFL dt is computed on the device (same expression, same IEEE square
 //     root and division as the driver, so the same dt), so nothing returns to
 //     the host inside a step.
@@ -76,9 +80,14 @@ struct GGBBatch {
     std::vector<Render *> r;
     std::vector<double> cfl, fade;
     std::vector<cudaStream_t> st;
-    std::vector<cudaEvent_t> ev_pre;
     double *dt_dev = nullptr;  // [n] device-side time steps
-    cudaEvent_t fork = nullptr, ev_solve = nullptr;
+    // the batched per-cell and per-particle stages
+    PlanetStepDev *steps_dev = nullptr;   // [n]
+    unsigned int *vmax_dev = nullptr;     // [n]
+    int4 *cell_map = nullptr, *part_map = nullptr;
+    int cell_blocks = 0, part_blocks = 0;
+    bool any_bfecc = false;
+    cudaEvent_t ev_solve = nullptr;
     // the batched solve
     GridBarrier *bars = nullptr;          // [n] one barrier per planet (zeroed before each launch)
     SolveParams *prm_host = nullptr;      // [n] pinned
@@ -253,15 +262,36 @@ GGB_EXPORT GGBBatch *ggb_batch_create(int n, Fluid *const *F, Particles *const *
         cudaStream_t s;
         GGB_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         b->st.push_back(s);
-        cudaEvent_t e;
-        GGB_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        b->ev_pre.push_back(e);
     }
     b->dt_dev = (double *)dev_alloc(sizeof(double) * n);
+    b->vmax_dev = (unsigned int *)dev_alloc(sizeof(unsigned int) * n);
+    // per-planet arguments and block maps of the batched stages (fixed for the batch)
+    {
+        std::vector<PlanetStepDev> st(n);
+        std::vector<int4> cm, pm;
+        for (int i = 0; i < n; i++) {
+            fluid_step_dev(b->F[i], b->cfl[i], b->dt_dev + i, b->vmax_dev + i, &st[i]);
+            particles_step_dev(b->P[i], &st[i]);
+            b->any_bfecc |= st[i].bfecc != 0;
+            const int cb = (int)batch_cell_blocks(b->F[i]->cs->ncells);
+            for (int k = 0; k < cb; k++) cm.push_back(make_int4(i, k, cb, 0));
+            if (st[i].np > 0) {
+                const int pb = (int)batch_particle_blocks(st[i].np);
+                for (int k = 0; k < pb; k++) pm.push_back(make_int4(i, k, pb, 0));
+            }
+        }
+        b->cell_blocks = (int)cm.size();
+        b->part_blocks = (int)pm.size();
+        b->steps_dev = (PlanetStepDev *)dev_alloc(sizeof(PlanetStepDev) * n);
+        b->cell_map = (int4 *)dev_alloc(sizeof(int4) * cm.size());
+        b->part_map = (int4 *)dev_alloc(sizeof(int4) * std::max<size_t>(1, pm.size()));
+        GGB_CHECK(cudaMemcpy(b->steps_dev, st.data(), sizeof(PlanetStepDev) * n, cudaMemcpyHostToDevice));
+        GGB_CHECK(cudaMemcpy(b->cell_map, cm.data(), sizeof(int4) * cm.size(), cudaMemcpyHostToDevice));
+        if (!pm.empty()) GGB_CHECK(cudaMemcpy(b->part_map, pm.data(), sizeof(int4) * pm.size(), cudaMemcpyHostToDevice));
+    }
     b->bars = (GridBarrier *)dev_alloc(sizeof(GridBarrier) * n);
     GGB_CHECK(cudaMallocHost(&b->prm_host, sizeof(SolveParams) * n));
     b->prm_dev = (SolveParams *)dev_alloc(sizeof(SolveParams) * n);
-    GGB_CHECK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     GGB_CHECK(cudaEventCreateWithFlags(&b->ev_solve, cudaEventDisableTiming));
     b->tune_steps = 4;
     sync();
@@ -293,20 +323,11 @@ GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
     refresh_params(b);
     for (int k = 0; k < steps; k++) {
         const auto t0 = clk::now();
-        // every planet's stream starts after the work already queued on the library stream
-        GGB_CHECK(cudaEventRecord(b->fork, base));
-        for (int i = 0; i < b->n; i++) {
-            GGB_CHECK(cudaStreamWaitEvent(b->st[i], b->fork, 0));
-            set_stream(b->st[i]);
-            Fluid *F = b->F[i];
-            fluid_cfl_dt_launch(F, b->cfl[i], b->dt_dev + i);
-            if (b->P[i]) particles_advect_queue(b->P[i], F->cs, F->vel, b->dt_dev + i);
-            fluid_advect_queue(F, b->dt_dev + i);
-            GGB_CHECK(cudaEventRecord(b->ev_pre[i], b->st[i]));
-        }
-        set_stream(nullptr);
-        // the batched solves, on the library stream after every planet's advection
-        for (int i = 0; i < b->n; i++) GGB_CHECK(cudaStreamWaitEvent(base, b->ev_pre[i], 0));
+        // CFL dt, particles and advection of every planet: one launch per stage
+        batch_cfl_launch(b->steps_dev, b->n, b->cell_map, b->cell_blocks, b->vmax_dev);
+        batch_particles_launch(b->steps_dev, b->part_map, b->part_blocks);
+        batch_advect_launch(b->steps_dev, b->cell_map, b->cell_blocks, b->any_bfecc);
+        // the batched solves
         GGB_CHECK(cudaMemsetAsync(b->bars, 0, sizeof(GridBarrier) * b->n, base));
         int q = 0;
         for (size_t g = 0; g < b->groups.size(); g++) {
@@ -317,18 +338,20 @@ GGB_EXPORT int ggb_batch_step(GGBBatch *b, int steps) {
                              base);
             q += nb;
         }
+        for (int i = 0; i < b->n; i++) fluid_result_queue(b->F[i]);
+        batch_velocity_launch(b->steps_dev, b->cell_map, b->cell_blocks);
         GGB_CHECK(cudaEventRecord(b->ev_solve, base));
+        // fade and splat per planet, each on its own stream
         for (int i = 0; i < b->n; i++) {
+            if (!b->r[i]) continue;
             GGB_CHECK(cudaStreamWaitEvent(b->st[i], b->ev_solve, 0));
             set_stream(b->st[i]);
-            fluid_result_velocity_queue(b->F[i]);
-            if (b->r[i]) {
-                render_fade(b->r[i], b->fade[i]);
-                if (b->P[i]) render_deposit_queue(b->r[i], b->P[i]);
-            }
+            render_fade(b->r[i], b->fade[i]);
+            if (b->P[i]) render_deposit_queue(b->r[i], b->P[i]);
         }
         set_stream(nullptr);
         const auto t1 = clk::now();
+        GGB_CHECK(cudaStreamSynchronize(base));
         for (int i = 0; i < b->n; i++) GGB_CHECK(cudaStreamSynchronize(b->st[i]));
         const auto t2 = clk::now();
         double smax = 0;
@@ -376,14 +399,16 @@ GGB_EXPORT void ggb_batch_free(GGBBatch *b) {
         cudaStreamDestroy(s);
     }
     sync();
-    for (cudaEvent_t e : b->ev_pre) cudaEventDestroy(e);
     dev_free(b->dt_dev);
+    dev_free(b->vmax_dev);
+    dev_free(b->steps_dev);
+    dev_free(b->cell_map);
+    dev_free(b->part_map);
     dev_free(b->bars);
     dev_free(b->prm_dev);
     dev_free(b->bmap_dev);
     cudaFreeHost(b->prm_host);
     cudaFreeHost(b->bmap_host);
-    cudaEventDestroy(b->fork);
     cudaEventDestroy(b->ev_solve);
     delete b;
 }

@@ -87,9 +87,9 @@ __global__ void k_remove_mean(int n, const double *part, int nparts, double tota
 }
 
 // u = p x sum_k gc_k (psi_j - psi_i); upstream src/fluid.c:361-376
-__global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *gc,
-                           const float *psi, float *vel) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void velocity_body(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *gc,
+                           const float *psi, float *vel, int vb_, int vnb_) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < n; i += vnb_ * blockDim.x) {
         D3 p = load3(pos + 3 * i), g = d3(0, 0, 0);
         double pi = psi[i];
         const int m = nnb[i];
@@ -118,14 +118,18 @@ __global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, co
         store3(vel + 3 * i, cross(p, g));
     }
 }
+__global__ void k_velocity(int n, const float *pos, const unsigned char *nnb, const int *nbr, const float *gc,
+                           const float *psi, float *vel) {
+    velocity_body(n, pos, nnb, nbr, gc, psi, vel, blockIdx.x, gridDim.x);
+}
 
 // max |u|^2 (formed in FP32 like upstream src/fluid.c:480-491) into *out as the
 // bits of a non-negative float, so that the unsigned atomicMax orders them; one
 // atomic per block.
-__global__ void __launch_bounds__(kB) k_max_speed2(int n, const float *vel, unsigned int *out) {
+__device__ __forceinline__ void max_speed2_body(int n, const float *vel, unsigned int *out, int vb_, int vnb_) {
     __shared__ float s_m[kB / 32];
     float m = 0.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < n; i += vnb_ * blockDim.x) {
         const float *v = vel + 3 * i;
         float s = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
         m = fmaxf(m, s);
@@ -138,6 +142,9 @@ __global__ void __launch_bounds__(kB) k_max_speed2(int n, const float *vel, unsi
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         if (threadIdx.x == 0) atomicMax(out, __float_as_uint(m));
     }
+}
+__global__ void __launch_bounds__(kB) k_max_speed2(int n, const float *vel, unsigned int *out) {
+    max_speed2_body(n, vel, out, blockIdx.x, gridDim.x);
 }
 
 // The application driver's CFL step on the device (upstream src/main.c:422-426):
@@ -162,11 +169,11 @@ __device__ __forceinline__ float q0_of(const float *omega, const float *pos, dou
 // kernel is writing; the sample point is the departure point as stored
 // (FP32), so q1 equals a separate resample of the stored q0 bit for bit.
 // dt: the time step, or *dtp when dtp is not null (a device-side CFL step).
-__global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt_in,
+__device__ __forceinline__ void departures_body(GridDev g, const float *pos, const float *vel, const float *omega, double dt_in,
                              const double *dtp, double two_omega, int forward, float *dep_b, float *dep_f,
-                             float *q0, float *q1) {
+                             float *q0, float *q1, int vb_, int vnb_) {
     const double dt = dtp ? *dtp : dt_in;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < g.n; i += vnb_ * blockDim.x) {
         D3 p = load3(pos + 3 * i), u = load3(vel + 3 * i);
         D3 pm = sphere_move(p, u, -0.5 * dt);
         D3 um = tangent(sample_vec(g, vel, pm), p);
@@ -185,11 +192,16 @@ __global__ void k_departures(GridDev g, const float *pos, const float *vel, cons
                         wt[2] * q0_of(omega, pos, two_omega, idx[2]) + wt[3] * q0_of(omega, pos, two_omega, idx[3]));
     }
 }
+__global__ void k_departures(GridDev g, const float *pos, const float *vel, const float *omega, double dt_in,
+                             const double *dtp, double two_omega, int forward, float *dep_b, float *dep_f,
+                             float *q0, float *q1) {
+    departures_body(g, pos, vel, omega, dt_in, dtp, two_omega, forward, dep_b, dep_f, q0, q1, blockIdx.x, gridDim.x);
+}
 
 // dst = src sampled at dep; with `correct`, dst = q0 + 0.5 (q0 - dst)
 // (the BFECC corrected source, upstream src/fluid.c:445-448).
-__global__ void k_resample(GridDev g, const float *src, const float *dep, const float *q0, int correct, float *dst) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void resample_body(GridDev g, const float *src, const float *dep, const float *q0, int correct, float *dst, int vb_, int vnb_) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < g.n; i += vnb_ * blockDim.x) {
         float v = (float)sample_scalar(g, src, load3(dep + 3 * i));
         if (correct) {
             float q = q0[i];
@@ -198,16 +210,19 @@ __global__ void k_resample(GridDev g, const float *src, const float *dep, const 
         dst[i] = v;
     }
 }
+__global__ void k_resample(GridDev g, const float *src, const float *dep, const float *q0, int correct, float *dst) {
+    resample_body(g, src, dep, q0, correct, dst, blockIdx.x, gridDim.x);
+}
 
 // Limited resample of the corrected source at dep_b (clamped to the range of
 // q0 over the same taps), then back to relative vorticity and relaxation
 // toward the band state.  upstream src/fluid.c:449-474
 // relax: the relaxation factor, or 1 - exp(-forcing *dtp) when dtp is not null.
-__global__ void k_limit_relax(GridDev g, const float *pos, const float *dep_b, const float *q0, const float *q2,
+__device__ __forceinline__ void limit_relax_body(GridDev g, const float *pos, const float *dep_b, const float *q0, const float *q2,
                               int bfecc, double two_omega, double relax_in, const double *dtp, double forcing,
-                              const float *omega_band, float *q1, float *omega) {
+                              const float *omega_band, float *q1, float *omega, int vb_, int vnb_) {
     const double relax = dtp ? (forcing > 0 ? 1.0 - exp(-forcing * *dtp) : 0.0) : relax_in;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < g.n; i += vnb_ * blockDim.x) {
         float qn;
         if (bfecc) {
             int idx[4];
@@ -232,6 +247,58 @@ __global__ void k_limit_relax(GridDev g, const float *pos, const float *dep_b, c
         w += relax * (omega_band[i] - w);
         omega[i] = (float)w;
     }
+}
+__global__ void k_limit_relax(GridDev g, const float *pos, const float *dep_b, const float *q0, const float *q2,
+                              int bfecc, double two_omega, double relax_in, const double *dtp, double forcing,
+                              const float *omega_band, float *q1, float *omega) {
+    limit_relax_body(g, pos, dep_b, q0, q2, bfecc, two_omega, relax_in, dtp, forcing, omega_band, q1, omega, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------- batched stages (all planets)
+// One launch per stage for every planet of a batch: block b runs the stage's
+// body for planet map[b].x as block map[b].y of map[b].z, with that planet's
+// arguments; the arithmetic per cell is the per-planet kernels'.
+
+__global__ void __launch_bounds__(kB) k_max_speed2_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    max_speed2_body(P.g.n, P.vel, P.vmax, m.y, m.z);
+}
+
+// dt of every planet (one thread each), k_cfl_dt's expression
+__global__ void k_cfl_dt_batch(const PlanetStepDev *pl, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PlanetStepDev &P = pl[i];
+    const double vmax = sqrt((double)__uint_as_float(*P.vmax));
+    *P.dt = P.cfl * P.g.h / (vmax > 1e-6 ? vmax : 1e-6);
+}
+
+__global__ void k_departures_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    departures_body(P.g, P.pos, P.vel, P.omega, 0.0, P.dt, P.two_omega, P.bfecc, P.dep_b, P.dep_f, P.q0, P.q1, m.y,
+                    m.z);
+}
+
+__global__ void k_resample_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    if (!P.bfecc) return;
+    resample_body(P.g, P.q1, P.dep_f, P.q0, 1, P.q2, m.y, m.z);
+}
+
+__global__ void k_limit_relax_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    limit_relax_body(P.g, P.pos, P.dep_b, P.q0, P.q2, P.bfecc, P.two_omega, 0.0, P.dt, P.forcing, P.omega_band, P.q1,
+                     P.omega, m.y, m.z);
+}
+
+__global__ void k_velocity_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    velocity_body(P.g.n, P.pos, P.nnb, P.nbr, P.gc, P.psi, P.vel, m.y, m.z);
 }
 
 // ------------------------------------------------------------ multigrid setup
@@ -334,7 +401,6 @@ struct FluidPriv {
     double *dense = nullptr;       // dense map of the V-cycle below the grid levels
     int nd = 0;
     int last_flags = 0;            // kSolve* bits of the last solve
-    int fuse_from = 2;             // SolveParams::fuse_from of this fluid's solves
     // mixed-precision solve (ggb_fluid_set_precision): FP16 level vectors,
     // FP16 slot weights of the coarse levels, the previous z
     int mixed = 0;
@@ -426,7 +492,6 @@ static SolveParams solve_params(Fluid *F, FluidPriv *Pv, int remove_mean, int ma
     const bool mg = F->prm.multigrid != 0;
     P.nlev = mg ? Pv->nlev : 0;
     P.coarse_sweeps = 60;
-    P.fuse_from = Pv->fuse_from;
     P.remove_mean = remove_mean;
     P.maxit = maxit;
     P.tol = F->prm.cg_tol;
@@ -680,16 +745,6 @@ GGB_EXPORT void fluid_free(Fluid *F) {
     memset(F, 0, sizeof(*F));
 }
 
-// The first multigrid level whose restriction is formed inside its pre-smooth
-// phase (see SolveParams::fuse_from); 0 turns the fusion off.  Returns the
-// previous value; a negative level only queries.
-GGB_EXPORT int ggb_fluid_fuse_from(Fluid *F, int level) {
-    FluidPriv *Pv = priv_of(F);
-    const int old = Pv->fuse_from;
-    if (level >= 0) Pv->fuse_from = level;
-    return old;
-}
-
 // Status bits of the last solve of F (kSolve* in ggb_solver.h; see ggb_ext.h).
 GGB_EXPORT int ggb_solve_flags(const Fluid *F) { return priv_of(F)->last_flags; }
 
@@ -829,6 +884,65 @@ void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks) {
 }
 
 void fluid_step_collect(Fluid *F) { solve_collect(F, priv_of(F)); }
+
+unsigned batch_cell_blocks(int n) { return blocks_for(n); }
+
+void fluid_step_dev(Fluid *F, double cfl, double *dt_dev, unsigned int *vmax_dev, PlanetStepDev *out) {
+    FluidPriv *Pv = priv_of(F);
+    const GridTables *t = Pv->grid0;
+    PlanetStepDev &d = *out;
+    d.g = t->dev();
+    d.pos = t->pos;
+    d.nnb = t->nnb;
+    d.nbr = t->nbr;
+    d.gc = t->gc;
+    d.vel = F->vel;
+    d.omega = F->omega;
+    d.omega_band = F->omega_band;
+    d.psi = F->psi;
+    d.q0 = F->q0;
+    d.q1 = F->q1;
+    d.q2 = F->q2;
+    d.dep_b = F->dep_b;
+    d.dep_f = F->dep_f;
+    d.two_omega = 2.0 * F->prm.rotation;
+    d.forcing = F->prm.forcing;
+    d.cfl = cfl;
+    d.bfecc = F->prm.bfecc != 0;
+    d.dt = dt_dev;
+    d.vmax = vmax_dev;
+}
+
+void batch_cfl_launch(const PlanetStepDev *pl, int n, const int4 *map, int nb, unsigned int *vmax_all) {
+    cudaStream_t s = stream();
+    GGB_CHECK(cudaMemsetAsync(vmax_all, 0, sizeof(unsigned int) * n, s));
+    k_max_speed2_batch<<<nb, kB, 0, s>>>(pl, map);
+    GGB_LAUNCHED();
+    k_cfl_dt_batch<<<grid_for(n, 128), 128, 0, s>>>(pl, n);
+    GGB_LAUNCHED();
+}
+
+void batch_advect_launch(const PlanetStepDev *pl, const int4 *map, int nb, bool any_bfecc) {
+    cudaStream_t s = stream();
+    k_departures_batch<<<nb, kB, 0, s>>>(pl, map);
+    GGB_LAUNCHED();
+    if (any_bfecc) {
+        k_resample_batch<<<nb, kB, 0, s>>>(pl, map);
+        GGB_LAUNCHED();
+    }
+    k_limit_relax_batch<<<nb, kB, 0, s>>>(pl, map);
+    GGB_LAUNCHED();
+}
+
+void batch_velocity_launch(const PlanetStepDev *pl, const int4 *map, int nb) {
+    k_velocity_batch<<<nb, kB, 0, stream()>>>(pl, map);
+    GGB_LAUNCHED();
+}
+
+void fluid_result_queue(Fluid *F) {
+    FluidPriv *Pv = priv_of(F);
+    GGB_CHECK(cudaMemcpyAsync(Pv->res_host, Pv->res, sizeof(SolveResult), cudaMemcpyDeviceToHost, stream()));
+}
 
 // The batched step around one batched solve launch: fluid_advect_queue, then
 // the solve (its parameters from fluid_step_solve_params; bar: the barrier the

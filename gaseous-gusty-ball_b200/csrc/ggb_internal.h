@@ -61,6 +61,39 @@ void stage_collect();  // after a stream sync: accumulate the recorded intervals
 void fluid_cfl_dt_launch(const Fluid *F, double cfl, double *dt_dev);
 void fluid_step_queue(Fluid *F, const double *dt_dev, int max_blocks);
 void fluid_step_collect(Fluid *F);
+// One planet's arguments of the batched per-cell and per-particle stages (one
+// launch per stage for all planets; each block finds its planet, its block of
+// that planet and the planet's block count in a block map of int4
+// {planet, block, blocks, 0}).
+struct PlanetStepDev {
+    GridDev g;                 // the planet's grid
+    const float *pos;          // [n*3] cell centres
+    const unsigned char *nnb;  // [n]
+    const int *nbr;            // [n*8]
+    const float *gc;           // [n*24]
+    float *vel, *omega, *omega_band, *psi, *q0, *q1, *q2, *dep_b, *dep_f;
+    double two_omega, forcing, cfl;
+    int bfecc;
+    double *dt;                // device-side time step of the planet
+    unsigned int *vmax;        // max |u|^2 as float bits
+    int np;                    // particles (0: none)
+    float *ppos, *pprev;
+};
+void fluid_step_dev(Fluid *F, double cfl, double *dt_dev, unsigned int *vmax_dev, PlanetStepDev *out);
+void particles_step_dev(Particles *P, PlanetStepDev *out);
+// The batched stages, queued on stream(): CFL dt (after zeroing the planets'
+// vmax), particle advection, departures + BFECC + limiter, velocity.  map:
+// block map of the planets' cells (nb blocks) or particles.
+void batch_cfl_launch(const PlanetStepDev *pl, int n, const int4 *map, int nb, unsigned int *vmax_all);
+void batch_particles_launch(const PlanetStepDev *pl, const int4 *map, int nb);
+void batch_advect_launch(const PlanetStepDev *pl, const int4 *map, int nb, bool any_bfecc);
+void batch_velocity_launch(const PlanetStepDev *pl, const int4 *map, int nb);
+// blocks of the per-cell (per-particle) stages for a planet of n cells (particles)
+unsigned batch_cell_blocks(int n);
+unsigned batch_particle_blocks(int n);
+// the result read-back of the last batched solve (fluid_result_velocity_queue without the velocity)
+void fluid_result_queue(Fluid *F);
+
 // The same step split around one batched solve launch (batch.cu): advection,
 // the solve's parameters (with the barrier the batched launch assigns), and
 // after the solve the result read-back and the velocity.

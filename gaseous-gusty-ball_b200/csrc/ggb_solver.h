@@ -50,11 +50,6 @@ struct SolveParams {
     int nlev_grid;       // non-coarsest levels 0..nlev_grid-1 run grid-wide
     int coarse_on_grid;  // coarsest level swept grid-wide (else by block 0)
     int coarse_sweeps;   // Jacobi sweeps on the coarsest level (upstream: 60)
-    int fuse_from;       // grid levels l >= fuse_from (l >= 1) form their right-hand side (the
-                         // restriction of level l-1's residual) while staging their pre-smooth,
-                         // and the dense map's blocks restrict its input themselves when
-                         // nlev_grid >= fuse_from: one phase and barrier fewer per level
-                         // (0 or > nlev_grid: every restriction is a phase of its own)
     int remove_mean;     // project the mean out of omega first
     int maxit;
     double tol;

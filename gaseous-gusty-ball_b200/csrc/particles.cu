@@ -57,11 +57,11 @@ __global__ void k_colour(int n, const float *pos, const float *img, int w, int h
     }
 }
 
-// RK2 midpoint step; upstream src/particles.c:63-74
-__global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *vel, double dt_in, const double *dtp,
-                                                float *pos, float *prev) {
+// RK2 midpoint step; upstream src/particles.c:63-74.  Over blocks vb_ of vnb_.
+__device__ __forceinline__ void advect_body(int n, const GridDev &g, const float *vel, double dt_in, const double *dtp,
+                                            float *pos, float *prev, int vb_, int vnb_) {
     const double dt = dtp ? *dtp : dt_in;  // *dtp: a device-side CFL step
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int i = vb_ * blockDim.x + threadIdx.x; i < n; i += vnb_ * blockDim.x) {
         float *pp = pos + 3 * (size_t)i;
         float p0 = pp[0], p1 = pp[1], p2 = pp[2];
         float *qq = prev + 3 * (size_t)i;
@@ -74,6 +74,34 @@ __global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *v
         D3 u2 = tangent(sample_vec(g, vel, pm), p);
         store3(pp, sphere_move(p, u2, dt));
     }
+}
+
+__global__ void __launch_bounds__(kPB) k_advect(int n, GridDev g, const float *vel, double dt_in, const double *dtp,
+                                                float *pos, float *prev) {
+    advect_body(n, g, vel, dt_in, dtp, pos, prev, blockIdx.x, gridDim.x);
+}
+
+// Every planet's particles in one launch (block map over the planets' particles).
+__global__ void __launch_bounds__(kPB) k_advect_batch(const PlanetStepDev *pl, const int4 *map) {
+    const int4 m = map[blockIdx.x];
+    const PlanetStepDev &P = pl[m.x];
+    advect_body(P.np, P.g, P.vel, 0.0, P.dt, P.ppos, P.pprev, m.y, m.z);
+}
+
+unsigned batch_particle_blocks(int n) { return blocks_for((size_t)n); }
+
+void particles_step_dev(Particles *P, PlanetStepDev *out) {
+    out->np = P ? P->n : 0;
+    out->ppos = P ? P->pos : nullptr;
+    out->pprev = P ? P->prev : nullptr;
+}
+
+void batch_particles_launch(const PlanetStepDev *pl, const int4 *map, int nb) {
+    if (nb <= 0) return;
+    stage_begin(ST_PARTICLES);
+    k_advect_batch<<<nb, kPB, 0, stream()>>>(pl, map);
+    GGB_LAUNCHED();
+    stage_end(ST_PARTICLES);
 }
 
 void particles_advect_launch(int n, const GridDev &g, const float *vel, double dt, const double *dtp, float *pos,

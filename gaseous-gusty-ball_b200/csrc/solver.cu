@@ -480,32 +480,6 @@ __device__ __forceinline__ void phase_presmooth(const LevelDev &L, const TB *b, 
     });
 }
 
-// Restriction F -> C fused with C's pre-smooth: b = R r_F (as stored) is formed
-// over the staged window of C from the fine residual, which is complete at the
-// start of the phase; the own cells' b is stored for C's post-smooth.  Same
-// values as a restriction phase followed by phase_presmooth, one grid barrier
-// fewer, at the price of restricting the window's halo cells as well.
-template <bool MP>
-__device__ __forceinline__ void phase_restrict_presmooth(const LevelDev &F, const LevelDev &C, double *buf) {
-    using A = typename Prec<MP>::A;
-    auto load = [&](int k, bool mine, Own &o) -> A {
-        const float bk = as_stored<MP>(restrict_value<MP>(F, C, k));
-        if (mine) o.a = bk;
-        return (A)presmooth_x<MP>(C, k, bk);
-    };
-    auto *cb = lv<MP>(C.b);
-    auto commit = [&](int k, const Own &o) { stv(cb, k, o.a); };
-    auto *lx = lv<MP>(C.x);
-    auto *lr = lv<MP>(C.r);
-    staged<MP>(C.S, buf, load, commit, [&](int c, STAGED_ARGS) {
-        const float bc = o.a;
-        const float xc = (float)x[c];  // = presmooth_x(C, c, bc)
-        const A kx = APPLY(C.S, c, (A)xc);
-        stv(lx, c, xc);
-        stv(lr, c, (float)(bc - kx));
-    });
-}
-
 // Prolongation C -> L fused with L's post-smooth: x = x_L + P xo_C is formed on
 // the fly over the staged window (never stored), then xo = x + w D^-1 (b - K x)
 // with b = bscale * b_in, stored as oscale * xo; returns sum dotr . (oscale xo)
@@ -563,7 +537,7 @@ struct SmemLevel {
     float *x, *xo, *b, *r;
 };
 
-__device__ __forceinline__ void carve_smem(const SolveParams &P, int l0, float *smem, SmemLevel *lv_) {
+__device__ void carve_smem(const SolveParams &P, int l0, float *smem, SmemLevel *lv_) {
     float *q = smem;
     for (int l = l0; l < P.nlev; l++) {
         int n = P.L[l].S.n;
@@ -668,26 +642,17 @@ __device__ __forceinline__ void vcycle_block_smem(const SolveParams &P, int l0, 
 // and visible; the V-cycle ran on s0 * r (s0 = 1 in the plain solve).  Ends
 // with rz = r . z (and, mixed, r . z_prev) published; returns false on abort.
 template <bool MP>
-__device__ __forceinline__ bool vcycle_rest(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
+__device__ bool vcycle_rest(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
                             double *s_red, double *buf, float *smem) {
     const int G = P.nlev_grid;
-    const int ff = P.fuse_from;
-    auto fused = [&](int l) { return ff >= 1 && l >= ff; };  // level l's restriction is inside its pre-smooth
     // down
     for (int l = 0; l < G; l++) {
         const LevelDev &L = P.L[l];
         if (l > 0) {
-            if (fused(l))
-                phase_restrict_presmooth<MP>(P.L[l - 1], L, buf);
-            else
-                phase_presmooth<MP>(L, lv<MP>(L.b), 1.0f, buf);
+            phase_presmooth<MP>(L, lv<MP>(L.b), 1.0f, buf);
             trace_mark(P, 100 + l);
             SYNC_OR(return false);
         }
-        // the restriction to level l+1: a phase of its own unless level l+1's
-        // pre-smooth (or, for the dense level, the dense map phase) does it
-        if (l + 1 < G && fused(l + 1)) continue;
-        if (l + 1 == G && P.dense && fused(G)) continue;
         GRID_LOOP(c, P.L[l + 1].S.n) restrict_cell<MP>(L, P.L[l + 1], c);
         trace_mark(P, 300 + l);
         SYNC_OR(return false);
@@ -695,33 +660,17 @@ __device__ __forceinline__ bool vcycle_rest(const SolveParams &P, const float *r
     // below the grid levels: the dense map, or block 0
     if (P.dense) {
         const LevelDev &C = P.L[G];
+        const auto *cb = lv<MP>(C.b);
+        auto *cx = lv<MP>(C.xo);
         const int nd = P.nd, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int gw = vb() * (blockDim.x >> 5) + warp, nw = vnb() * (blockDim.x >> 5);
-        auto *cx = lv<MP>(C.xo);
-        if (fused(G)) {
-            // every block restricts the whole input of the map (nd <= 1536 cells)
-            // into shared memory itself instead of waiting for a restriction phase
-            float *sb = reinterpret_cast<float *>(buf);
-            BLOCK_LOOP(j, nd) sb[j] = as_stored<MP>(restrict_value<MP>(P.L[G - 1], C, j));
-            __syncthreads();
-            for (int row = gw; row < nd; row += nw) {
-                const double *d = P.dense + (size_t)row * nd;
-                double acc = 0;
-                for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)sb[j];
+        for (int row = gw; row < nd; row += nw) {
+            const double *d = P.dense + (size_t)row * nd;
+            double acc = 0;
+            for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)ldv(cb, j);
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) stv(cx, row, (float)acc);
-            }
-        } else {
-            const auto *cb = lv<MP>(C.b);
-            for (int row = gw; row < nd; row += nw) {
-                const double *d = P.dense + (size_t)row * nd;
-                double acc = 0;
-                for (int j = lane; j < nd; j += 32) acc += __ldg(d + j) * (double)ldv(cb, j);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) stv(cx, row, (float)acc);
-            }
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) stv(cx, row, (float)acc);
         }
         trace_mark(P, 500);
         SYNC_OR(return false);
@@ -781,7 +730,7 @@ __device__ __forceinline__ bool vcycle_rest(const SolveParams &P, const float *r
 // z = V(r) for a single-level hierarchy (level 0 is the coarsest grid); the
 // sweeps run on s0 * r (s0 = 1 in the plain solve).
 template <bool MP>
-__device__ __forceinline__ bool single_level(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
+__device__ bool single_level(const SolveParams &P, const float *r, float s0, float *z, const float *zold,
                              double *s_red, float *smem) {
     const LevelDev &L = P.L[0];
     auto *lx = lv<MP>(L.x), *lxo = lv<MP>(L.xo);

@@ -135,15 +135,6 @@ int ggb_remove_mean_noalloc(const CubeSphere *cs, float *f);
  * the choice is made here rather than there. */
 int ggb_fluid_set_precision(Fluid *F, int mixed);
 
-/* Schedule of F's multigrid solve: coarse levels from `level` on (level >= 1)
- * form their right-hand side, the restriction of the finer level's residual,
- * inside their pre-smooth phase, and the dense coarse map's blocks restrict
- * its input themselves, which saves a grid-wide barrier per level at the
- * price of restricting each block's halo cells as well; 0 makes every
- * restriction a phase of its own.  The values computed are the same either
- * way.  Returns the previous setting (level < 0: query only). */
-int ggb_fluid_fuse_from(Fluid *F, int level);
-
 /* Checkpoint / resume of a running planet.  save writes the state the next
  * steps read (omega, omega_band, psi, vel and the last solve's statistics; the
  * particles' pos, prev, col; the face buffer, g and a deferred fade
