@@ -31,6 +31,7 @@
 namespace ggb {
 
 constexpr int kT = 16;              // tile edge in texels
+constexpr unsigned kTileSpare = 64;  // spare record slots of a tile whose reservation is estimated
 constexpr int kMaxSamples = 4096;   // upstream cap on samples per arc
 
 // One splat sample on one tile: its compositing order key (particle index
@@ -402,7 +403,7 @@ __global__ void __launch_bounds__(256, 5)
 // reserves that count plus half of it plus 32 (records of a tile change little
 // from one step to the next; a tile that still overflows makes the deposit
 // repeat with exact reservations).
-__device__ __forceinline__ unsigned tile_reserve(unsigned x, int est) { return est ? x + x / 2 + 32u : x; }
+__device__ __forceinline__ unsigned tile_reserve(unsigned x, int est) { return est ? x + x / 2 + kTileSpare : x; }
 
 // Counts i..i+3 (zero past n), transformed by tile_reserve.
 __device__ __forceinline__ uint4 tile_load4(const unsigned *cnt, int i, int n, int est) {
@@ -584,12 +585,19 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
     return total;
 }
 
-// Record r with its box and its particle's colour into slot s of the current window.
-__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box, const float4 *col) {
+// Record r with its box into slot s of the current window (its particle's
+// colour: window_colours).
+__device__ __forceinline__ void window_put(TileSmem &S, int s, const Rec &r, unsigned short box) {
     S.u.r.key[s] = r.key;
     S.u.r.pos[s] = make_float2(r.px, r.py);
     S.box[s] = box;
-    S.col[s] = __ldg(col + (r.key >> 13));
+}
+
+// The colours of the window's records 0..m-1, gathered by the particle index
+// in each key after the records are binned, so that a thread's gathers are in
+// flight together instead of one per record on the binning loop's path.
+__device__ __forceinline__ void window_colours(TileSmem &S, int m, const float4 *col) {
+    for (int s = threadIdx.x; s < m; s += blockDim.x) S.col[s] = __ldg(col + (S.u.r.key[s] >> 13));
 }
 
 // Blends the sorted entries e[0..m) of texel q into d (upstream
@@ -744,10 +752,12 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, const float4 *col,
             const unsigned short box = rec_box(C, G, r.px, r.py);
             if (box == kNoBox) continue;
             const int slot = atomicAdd(&S.cut, 1);
-            if (slot < kRec) window_put(S, slot, r, box, col);
+            if (slot < kRec) window_put(S, slot, r, box);
         }
         __syncthreads();
         const int nw = min(S.cut, kRec);
+        window_colours(S, nw, col);
+        __syncthreads();
         composite_window(S, nw, C, G, d);
         lo = hi;
     }
@@ -802,7 +812,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
             for (int s = q; s < m; s += kTB) {
                 const Rec r = Rt[s];
                 const unsigned short box = rec_box(C, G, r.px, r.py);
-                window_put(S, s, r, box, col);
+                window_put(S, s, r, box);
                 box_texels(box, [&](int t) {
                     const int k = atomicAdd(&S.cnt[t], 1);
                     if (k < kBucket)
@@ -815,6 +825,7 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
             if ((q & 31) == 0 && e) atomicAdd(&S.tot, e);
+            window_colours(S, m, col);  // each thread reads back the keys it stored itself
         }
         __syncthreads();
         if (m <= kRec && !S.full) {
@@ -905,11 +916,17 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
 // compositing skips it when an estimated tile overflowed.  The host then grows
 // the buffer and runs them again on the same reservations, or repeats the
 // deposit with exact reservations.
+static void grow_records(RenderPriv *Pv, size_t need);
+
 void render_deposit_queue(Render *r, const Particles *P) {
     RenderPriv *Pv = rpriv(r);
     cudaStream_t s = stream();
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
+    // the first deposit's records are not known before its fill: size the
+    // buffer for six per particle (the default workload makes about 4.3), so
+    // that the fill does not have to run a second time on a grown buffer
+    if (!Pv->have_prev) grow_records(Pv, (size_t)6 * n);
     // estimated reservations unless a recent estimate overflowed (a sparse
     // planet's tile counts can jump from one step to the next; each overflow
     // costs a repeated deposit, each exact reservation only the counting pass)
@@ -944,12 +961,12 @@ void render_deposit_queue(Render *r, const Particles *P) {
 
 // Grows the record buffer to hold need records, with room for the next
 // deposit's estimated reservation (at most 1.5 x this deposit's records plus
-// 32 per tile).  Without that room a sparse planet, whose estimate is mostly
-// the 32 slots per tile, would outgrow the buffer at every deposit.
+// kTileSpare per tile).  Without that room a sparse planet, whose estimate is
+// mostly the spare slots, would outgrow the buffer at every deposit.
 static void grow_records(RenderPriv *Pv, size_t need) {
     if (need <= Pv->rec_cap) return;
     dev_free(Pv->recs);
-    Pv->rec_cap = need + need / 2 + (size_t)32 * Pv->ntiles + 1024;
+    Pv->rec_cap = need + need / 2 + (size_t)kTileSpare * Pv->ntiles + 1024;
     Pv->recs = (Rec *)dev_alloc(sizeof(Rec) * Pv->rec_cap);
 }
 

@@ -663,7 +663,7 @@ def test_batched_step_fluid_only_planet(gpu):
 def test_deposit_estimated_reservation_overflow_repeats(gpu, orc32):
     """After a first deposit, each tile reserves slots from that deposit's
     record counts.  A second deposit that packs 3000 particles into tiles the
-    first left empty (32 slots each) overflows them; the library repeats it
+    first left empty (64 spare slots each) overflows them; the library repeats it
     with exact reservations, so the faces equal the restatement's."""
     R = 48
     prev_a, pos_a, col_a = K.random_arcs(200, seed=31, max_angle=0.02)
@@ -717,9 +717,9 @@ def test_deposit_overflow_backoff(gpu, orc32):
     col_b = rng.uniform(0.1, 1, size=(3000, 4))
     # deposit:           a  b  a  b  a  b  a  b
     # reservation:       x  e  x  e  x  x  e  e   (x exact, e estimated)
-    # repeats: the first deposit grows the record buffer, every estimated b
-    # overflows (cumulative count after each deposit)
-    expect_repeats = [1, 2, 2, 3, 3, 3, 3, 4]
+    # repeats: every estimated b overflows (cumulative count after each
+    # deposit; the first deposit sizes the record buffer before its fill)
+    expect_repeats = [0, 1, 1, 2, 2, 2, 2, 3]
     out = {}
     for name, api in (("gpu", gpu), ("orc", orc32)):
         sets = []
