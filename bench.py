@@ -368,10 +368,12 @@ def run_ours(a, rank, world, local):
     clk, clk_path = start_clock_sampler(local)
     time.sleep(0.3)
     l0 = api.lib.ggb_launch_count()
+    rep0 = api.lib.ggb_render_repeats(C.byref(pl.sp.r))
     api.lib.ggb_timer_start()
     its = [pl.step() for _ in range(K)]
     ms = api.lib.ggb_timer_stop()
     launches = api.lib.ggb_launch_count() - l0
+    rep_timed = api.lib.ggb_render_repeats(C.byref(pl.sp.r)) - rep0
     clocks = stop_clock_sampler(clk, clk_path)
     barrier()
     ms = max_over_ranks(ms)
@@ -457,7 +459,10 @@ def run_ours(a, rank, world, local):
                                     "plain: FP32 vectors, FP64 stencil sums, FP64 dots / norms / mean projections",
                        "l2": working_set_note(CFG),
                        "mean_cg_iters": kit,
-                       "deposit_repeats": int(api.lib.ggb_render_repeats(C.byref(pl.sp.r))),
+                       "deposit_repeats": {"timed": int(rep_timed),
+                                           "run": int(api.lib.ggb_render_repeats(C.byref(pl.sp.r))),
+                                           "run_after_buffer_growth":
+                                               int(api.lib.ggb_render_repeats_grown(C.byref(pl.sp.r)))},
                        "stage_ms_per_step": {k: v[0] / KS for k, v in per_stage.items()},
                        "stage_steps": KS},
             "e2e": {"value": e2e, "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -639,25 +644,34 @@ def run_batch(a, rank, world, local):
     its, solve_ms = [], []
     half = max(1, K // 2)
     launches_b = 0
+
+    def repeats():
+        return sum(api.lib.ggb_render_repeats(C.byref(p[3].r)) for p in planets)
+
+    rep_b = rep_p = 0
     for seg in range(2):
         set_precision(mixed)
         barrier()
         lb = api.lib.ggb_launch_count()
+        r0 = repeats()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
         api.lib.ggb_batch_step(b, half)
         ms_b += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
         launches_b += api.lib.ggb_launch_count() - lb
+        rep_b += repeats() - r0
         its += [p[1].F.cg_iters for p in planets]
         solve_ms.append(api.lib.ggb_batch_solve_ms(b))
         set_precision(False)
         barrier()
+        r0 = repeats()
         api.lib.ggb_timer_start()
         t0 = time.perf_counter()
         for _ in range(half):
             for p in planets:
                 plain_step(p)
         ms_p += max_over_ranks(max(api.lib.ggb_timer_stop(), 1000 * (time.perf_counter() - t0)))
+        rep_p += repeats() - r0
     clocks = stop_clock_sampler(clk, clk_path)
     K = 2 * half
     # one more batched step: the state the FP64 check below solves again
@@ -703,7 +717,10 @@ def run_batch(a, rank, world, local):
                        "solve_blocks_by_N": shares, "tuned_cost_s_per_cell_block": tuned,
                        "batched_solve_ms_last_step": solve_ms,
                        "host_ms_last_step": host_ms,
-                       "deposit_repeats": int(sum(api.lib.ggb_render_repeats(C.byref(p[3].r)) for p in planets)),
+                       "deposit_repeats": {
+                           "timed_batched": int(rep_b), "timed_plain": int(rep_p), "run": int(repeats()),
+                           "run_after_buffer_growth":
+                               int(sum(api.lib.ggb_render_repeats_grown(C.byref(p[3].r)) for p in planets))},
                        "timing": "max of CUDA events on the library stream and the host wall clock"},
             "cpu_baseline": base,
             "gpu_launches": int(launches_b),

@@ -132,6 +132,7 @@ GGB_EXPORT int ggb_checkpoint_load(const char *path, Fluid *F, Particles *P, Ren
     if (r) {
         r->g = h.g;
         render_pending_set(r, h.pending, h.pending_scale);
+        if (P) render_particles_replaced(r);
     }
     sync();
     return 0;

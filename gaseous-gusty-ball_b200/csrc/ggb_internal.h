@@ -114,6 +114,7 @@ void particles_advect_queue(Particles *P, const CubeSphere *cs, const float *vel
 // The deferred renormalisation of render_fade (private state of a Render).
 void render_pending_get(const Render *r, int *pending, float *scale);
 void render_pending_set(Render *r, int pending, float scale);
+void render_particles_replaced(Render *r);
 
 void *dev_alloc(size_t bytes);      // cudaMalloc, zero-filled; exits on failure
 void dev_free(void *p);

@@ -66,6 +66,7 @@ struct RenderPriv {
     bool queued_est = false;       // its slots were estimated from the previous deposit's fills
     bool have_prev = false;        // tile_fill holds the previous deposit's record counts
     unsigned long repeats = 0;     // times a deposit's fill and compositing ran again
+    unsigned long grown = 0;       // of those, after the record buffer grew
     int exact_next = 0;            // deposits still to reserve exactly after an estimate overflowed
     int backoff = 1;               // exact deposits after the next overflow (doubles up to 64)
     float *mirror = nullptr;
@@ -976,6 +977,7 @@ static void grow_records(RenderPriv *Pv, size_t need) {
 static unsigned deposit_refill(Render *r, const Particles *P, RenderPriv *Pv) {
     cudaStream_t s = stream();
     Pv->repeats++;
+    Pv->grown++;
     GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
     deposit_fill_tiles(r, P, Pv, Pv->queued);
@@ -1063,6 +1065,14 @@ void render_pending_set(Render *r, int pending, float scale) {
     Pv->pending = pending != 0;
     Pv->pending_scale = pending ? scale : 1.f;
     Pv->dev_gen++;
+}
+
+// The particles were replaced (a checkpoint restore): the previous deposit's
+// per-tile record counts describe other positions, so the next deposit
+// reserves exactly instead of from them.
+void render_particles_replaced(Render *r) {
+    RenderPriv *Pv = rpriv(r);
+    if (Pv->have_prev) Pv->exact_next = std::max(Pv->exact_next, 1);
 }
 
 // ---- 8-bit output encoding (upstream src/main.c:249-318) --------------------
@@ -1383,6 +1393,7 @@ GGB_EXPORT void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *sl
 // Render's deposits ran again (record buffer grown, or an estimated tile
 // reservation overflowed).
 GGB_EXPORT unsigned long ggb_render_repeats(const Render *r) { return rpriv(r)->repeats; }
+GGB_EXPORT unsigned long ggb_render_repeats_grown(const Render *r) { return rpriv(r)->grown; }
 
 // Additive: the application driver's 8-bit images, encoded on the GPU (upstream
 // src/main.c:249-318).  bg == NULL: transparent (RGBA, un-premultiplied);

@@ -144,6 +144,7 @@ class Api:
             ("ggb_render_read", None, [P(T["Render"]), R]),
             ("ggb_render_stats", None, [P(T["Render"]), P(C.c_uint), P(C.c_uint), P(C.c_uint)]),
             ("ggb_render_repeats", C.c_ulong, [P(T["Render"])]),
+            ("ggb_render_repeats_grown", C.c_ulong, [P(T["Render"])]),
             ("ggb_encode_faces", C.c_int, [P(T["Render"]), P(C.c_float), P(C.c_int), P(C.c_ubyte)]),
             ("ggb_encode_net", C.c_int, [P(T["Render"]), P(C.c_float), P(C.c_ubyte)]),
             ("ggb_checkpoint_save", C.c_int, [C.c_char_p, P(T["Fluid"]), P(T["Particles"]), P(T["Render"])]),

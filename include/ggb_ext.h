@@ -88,6 +88,9 @@ void ggb_render_stats(const Render *r, unsigned *ntiles, unsigned *slow_tiles, u
  * deposits ran again (the record buffer grew, or a tile outgrew its estimated
  * reservation). */
 unsigned long ggb_render_repeats(const Render *r);
+/* Of ggb_render_repeats, those that followed a growth of the record buffer
+ * (the others followed a tile that outgrew its estimated reservation). */
+unsigned long ggb_render_repeats_grown(const Render *r);
 
 /* The application driver's 8-bit output images (its write_outputs), encoded
  * on the GPU from the face buffer: render_texel then render_pixel8 per texel.

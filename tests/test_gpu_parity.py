@@ -473,6 +473,17 @@ def test_checkpoint_resume(gpu, tmp_path):
     got = state(*b)
     for k in want:
         assert np.array_equal(np.asarray(got[k]), np.asarray(want[k])), k
+    # restored into the object that made the file, whose last deposit's tile
+    # counts describe later positions: the next deposit reserves exactly, so
+    # the replay repeats no deposit and reaches the same state
+    rep0 = int(gpu.lib.ggb_render_repeats(C.byref(a[3].r)))
+    assert gpu.lib.ggb_checkpoint_load(path, C.byref(a[1].F), C.byref(a[2].P), C.byref(a[3].r)) == 0
+    for _ in range(3):
+        step(*a)
+    assert int(gpu.lib.ggb_render_repeats(C.byref(a[3].r))) == rep0
+    again = state(*a)
+    for k in want:
+        assert np.array_equal(np.asarray(again[k]), np.asarray(want[k])), k
     # a mismatched object is refused
     c = G.ParticleSet(gpu, npart + 1)
     assert gpu.lib.ggb_checkpoint_load(path, C.byref(b[1].F), C.byref(c.P), C.byref(b[3].r)) == -1
