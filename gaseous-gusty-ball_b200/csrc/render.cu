@@ -56,6 +56,7 @@ struct SplatCfg {
 struct RenderPriv {
     int R = 0, ntx = 0, ntiles = 0;
     unsigned *tile_count = nullptr, *tile_start = nullptr, *tile_fill = nullptr;
+    unsigned *tile_est = nullptr;  // next deposit's estimate: neighbourhood maxima of the record counts
     Rec *recs = nullptr;
     size_t rec_cap = 0;
     unsigned *diag = nullptr;        // device: [0] windowed tiles of the last deposit, [1] tiles whose slots overflowed
@@ -399,11 +400,16 @@ __global__ void __launch_bounds__(256, 5)
 // 128 long; cnt and start are 16-byte aligned) and walks it 128 counts at a
 // time, a 16-byte load per lane (coalesced): a first pass sums the segment,
 // the block scans the 32 warp sums, a second pass writes the prefixes (a warp
-// scan per step, the running total carried from step to step).
-// est: the counts are the previous deposit's record counts, and each tile
-// reserves that count plus half of it plus 32 (records of a tile change little
-// from one step to the next; a tile that still overflows makes the deposit
-// repeat with exact reservations).
+// scan per step, the running total carried from step to step); the second
+// pass also zeroes clear[0..n) (the estimate array, which the following
+// compositing fills for the next deposit; clear may be cnt).
+// est: the counts are the previous deposit's estimates (for each tile the
+// largest record count among the tile and its neighbours on the same face,
+// left by k_rd_tiles), and each tile reserves that plus half of it plus
+// kTileSpare (a particle moves up to one grid cell per step, which on a
+// coarse grid under large faces is a whole tile, so a dense stream's records
+// can move into a tile that held few of them; a tile that still overflows
+// makes the deposit repeat with exact reservations).
 __device__ __forceinline__ unsigned tile_reserve(unsigned x, int est) { return est ? x + x / 2 + kTileSpare : x; }
 
 // Counts i..i+3 (zero past n), transformed by tile_reserve.
@@ -427,7 +433,7 @@ __device__ __forceinline__ uint4 tile_load4(const unsigned *cnt, int i, int n, i
 }
 
 __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, int est, unsigned *start,
-                                                   unsigned *total) {
+                                                   unsigned *total, unsigned *clear) {
     __shared__ unsigned s_w[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int seg = ((n + 31) / 32 + 127) & ~127;
@@ -461,6 +467,11 @@ __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, 
     for (int b = w0; b < w1; b += 128) {
         const int i = b + 4 * lane;
         const uint4 v = tile_load4(cnt, i, w1, est);
+        if (i + 4 <= w1) {  // clear may be cnt itself: these entries were read just above
+            reinterpret_cast<uint4 *>(clear)[i >> 2] = make_uint4(0u, 0u, 0u, 0u);
+        } else {
+            for (int u = i; u < w1 && u < i + 4; u++) clear[u] = 0u;
+        }
         const unsigned t = v.x + v.y + v.z + v.w;
         unsigned incl = t;
 #pragma unroll
@@ -769,7 +780,8 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, const float4 *col,
 // registers left room for.
 __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned *tile_start,
                                                   const unsigned *tile_fill, const Rec *recs, size_t cap,
-                                                  const float4 *col, float *buf, unsigned *diag) {
+                                                  const float4 *col, float *buf, unsigned *diag,
+                                                  unsigned *est_next) {
     if (tile_start[C.ntiles] > cap) return;  // records not filled: see k_rd_fill
     if (diag[1]) return;                     // a tile's records overflowed: the deposit is repeated
     __shared__ TileSmem S;
@@ -853,6 +865,14 @@ __global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned 
         }
     }
     if (inside) face[(size_t)(G.y0 + ly) * R + G.x0 + lx] = d;
+    // the next deposit's estimate of this tile and its neighbours on the face
+    // (nine threads, one neighbour each; the count is read again here so that
+    // it need not stay in a register through the compositing)
+    if (q < 9) {
+        const int y = ty + q / 3 - 1, x = tx + q % 3 - 1;
+        const unsigned mm = min(__ldg(tile_fill + tile), __ldg(tile_start + tile + 1) - s0);
+        if (mm > 0 && y >= 0 && y < ntx && x >= 0 && x < ntx) atomicMax(est_next + (f * ntx + y) * ntx + x, mm);
+    }
 }
 
 // Buffer renormalisation on its own (a second renormalisation falling due
@@ -900,7 +920,7 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
         GGB_LAUNCHED();
     }
     k_rd_tiles<<<Pv->ntiles, kTB, 0, s>>>(C, Pv->tile_start, Pv->tile_fill, Pv->recs, Pv->rec_cap,
-                                          reinterpret_cast<const float4 *>(P->col), r->buf, Pv->diag);
+                                          reinterpret_cast<const float4 *>(P->col), r->buf, Pv->diag, Pv->tile_est);
     GGB_LAUNCHED();
     stage_end(ST_TILES);
 }
@@ -908,7 +928,7 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
 // The whole deposit without a host round trip: queues the slot reservation,
 // scan, fill and compositing and the copies of the reserved total and the
 // overflow count.  The reservation is exact (k_rd_count) for the first deposit
-// and estimated from the previous deposit's per-tile record counts afterwards
+// and estimated from the previous deposit's per-tile record counts (neighbourhood maxima) afterwards
 // (no counting pass), except for the b deposits after an estimate overflowed
 // (b doubles with every overflow up to 64 and halves with every estimate that
 // fits).  render_deposit_collect (after a synchronisation of the
@@ -925,9 +945,10 @@ void render_deposit_queue(Render *r, const Particles *P) {
     SplatCfg C = splat_cfg(r, Pv);
     int n = P->n;
     // the first deposit's records are not known before its fill: size the
-    // buffer for six per particle (the default workload makes about 4.3), so
-    // that the fill does not have to run a second time on a grown buffer
-    if (!Pv->have_prev) grow_records(Pv, (size_t)6 * n);
+    // buffer for eight per particle (the default workload makes about 4.3, and
+    // the next deposit's neighbourhood estimate reserves about 2.5 times its
+    // records), so that neither fill has to run a second time on a grown buffer
+    if (!Pv->have_prev) grow_records(Pv, (size_t)8 * n);
     // estimated reservations unless a recent estimate overflowed (a sparse
     // planet's tile counts can jump from one step to the next; each overflow
     // costs a repeated deposit, each exact reservation only the counting pass)
@@ -936,7 +957,8 @@ void render_deposit_queue(Render *r, const Particles *P) {
     stage_begin(ST_BIN);
     GGB_CHECK(cudaMemsetAsync(Pv->diag, 0, 2 * sizeof(unsigned), s));
     if (est) {
-        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_fill, 1, Pv->tile_start, Pv->tile_count + Pv->ntiles);
+        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_est, 1, Pv->tile_start, Pv->tile_count + Pv->ntiles,
+                                       Pv->tile_est);
         GGB_LAUNCHED();
     } else {
         GGB_CHECK(cudaMemsetAsync(Pv->tile_count, 0, sizeof(unsigned) * Pv->ntiles, s));
@@ -945,7 +967,8 @@ void render_deposit_queue(Render *r, const Particles *P) {
             k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
             GGB_LAUNCHED();
         }
-        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles);
+        k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles,
+                                       Pv->tile_est);
         GGB_LAUNCHED();
     }
     GGB_CHECK(cudaMemsetAsync(Pv->tile_fill, 0, sizeof(unsigned) * Pv->ntiles, s));
@@ -961,9 +984,10 @@ void render_deposit_queue(Render *r, const Particles *P) {
 }
 
 // Grows the record buffer to hold need records, with room for the next
-// deposit's estimated reservation (at most 1.5 x this deposit's records plus
-// kTileSpare per tile).  Without that room a sparse planet, whose estimate is
-// mostly the spare slots, would outgrow the buffer at every deposit.
+// deposit's estimated reservation (1.5 x the neighbourhood maxima of this
+// deposit's counts plus kTileSpare per tile, about as much as this one's).
+// Without that room a sparse planet, whose estimate is mostly the spare
+// slots, would outgrow the buffer at every deposit.
 static void grow_records(RenderPriv *Pv, size_t need) {
     if (need <= Pv->rec_cap) return;
     dev_free(Pv->recs);
@@ -1000,7 +1024,8 @@ static void deposit_exact(Render *r, const Particles *P, RenderPriv *Pv) {
         k_rd_count<<<nb, 256, 0, s>>>(n, C, P->prev, P->pos, Pv->tile_count);
         GGB_LAUNCHED();
     }
-    k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles);
+    k_tile_scan<<<1, 1024, 0, s>>>(Pv->ntiles, Pv->tile_count, 0, Pv->tile_start, Pv->tile_count + Pv->ntiles,
+                                   Pv->tile_est);
     GGB_LAUNCHED();
     GGB_CHECK(cudaMemcpyAsync(Pv->total_host, Pv->tile_count + Pv->ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     GGB_CHECK(cudaStreamSynchronize(s));
@@ -1265,6 +1290,7 @@ GGB_EXPORT int render_init(Render *r, int R, float radius, float alpha) {
     Pv->tile_count = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_start = (unsigned *)dev_alloc(sizeof(unsigned) * (Pv->ntiles + 1));
     Pv->tile_fill = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);
+    Pv->tile_est = (unsigned *)dev_alloc(sizeof(unsigned) * Pv->ntiles);  // zeroed
     Pv->diag = (unsigned *)dev_alloc(sizeof(unsigned) * 2);  // zeroed
     GGB_CHECK(cudaMallocHost(&Pv->total_host, sizeof(unsigned) * 2));
     Pv->total_host[0] = Pv->total_host[1] = 0;
@@ -1280,6 +1306,7 @@ GGB_EXPORT void render_free(Render *r) {
         dev_free(Pv->tile_count);
         dev_free(Pv->tile_start);
         dev_free(Pv->tile_fill);
+        dev_free(Pv->tile_est);
         dev_free(Pv->diag);
         dev_free(Pv->recs);
         cudaFreeHost(Pv->total_host);
