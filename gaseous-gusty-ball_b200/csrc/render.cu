@@ -49,6 +49,7 @@ struct SplatCfg {
     int R, ntx, ntiles;
     float rad, invrad, invg, alpha;
     double spacing;
+    double edge_lim;  // 1 + (2 rad + 2) / R: beyond |u| or |v| of that a face's footprint is empty
     int renorm;
     float scale;
 };
@@ -375,18 +376,23 @@ __global__ void __launch_bounds__(256, 5)
                 const float py = (float)__fma_rn((1.0 - v) * 0.5, (double)C.R, -0.5);
                 emit_face(C, f0, px, py, live, key, tile_start, tile_fill, recs, diag);
             }
-            // other faces with d.c >= 0.5 (cube edges and corners)
-            bool more = false;
+            // other faces with d.c >= 0.5 (cube edges and corners) whose texels
+            // the sample reaches: its footprint on face f is empty unless
+            // -rad <= px <= R - 1 + rad, i.e. |u|, |v| <= 1 + (2 rad + 1) / R;
+            // edge_lim adds 1 / R for rounding and the test multiplies by
+            // d.c instead of dividing.  Faces it skips make no records.
+            unsigned reach = 0;
 #pragma unroll
             for (int f = 0; f < 6; f++) {
                 double ec, er, eu;
                 face_proj(f, d, ec, er, eu);
-                more |= f != f0 && ec >= 0.5;
+                const double lim = C.edge_lim * ec;
+                if (f != f0 && ec >= 0.5 && fabs(er) <= lim && fabs(eu) <= lim) reach |= 1u << f;
             }
-            if (__any_sync(0xffffffffu, live && more)) {
+            if (__any_sync(0xffffffffu, live && reach)) {
                 for (int f = 0; f < 6; f++) {
                     float px = 0.f, py = 0.f;
-                    const bool on = live && f != f0 && face_px(f, d, C.R, px, py);
+                    const bool on = live && (reach >> f & 1u) && face_px(f, d, C.R, px, py);
                     if (__any_sync(0xffffffffu, on))
                         emit_face(C, f, px, py, on, key, tile_start, tile_fill, recs, diag);
                 }
@@ -892,6 +898,7 @@ static SplatCfg splat_cfg(const Render *r, const RenderPriv *Pv) {
     C.invg = (float)(1.0 / r->g);
     C.alpha = r->alpha;
     C.spacing = 0.7 / r->R;
+    C.edge_lim = 1.0 + (2.0 * (double)r->radius + 2.0) / r->R;
     C.renorm = Pv->pending ? 1 : 0;
     C.scale = Pv->pending_scale;
     return C;
