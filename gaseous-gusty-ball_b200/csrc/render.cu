@@ -503,8 +503,8 @@ __global__ void __launch_bounds__(1024) k_tile_scan(int n, const unsigned *cnt, 
 
 // ---- tile compositing: one block per tile, one texel per thread ----------
 constexpr int kTB = kT * kT;   // threads per tile block: one texel each
-constexpr int kRec = 768;      // records of one window (shared memory)
-constexpr int kEnt = 2304;     // (record, texel) entries of one window
+constexpr int kRec = 576;      // records of one window (shared memory)
+constexpr int kEnt = 1728;     // (record, texel) entries of one window
 constexpr int kHist = 1024;    // key buckets when a dense tile is cut into windows
 constexpr int kBucket = 16;    // entry slots per texel of the one-pass path
 constexpr int kBucketStride = 18;  // slots between texels: 9 words, so a warp's texels hit distinct banks
@@ -781,10 +781,10 @@ __device__ void composite_windowed(TileSmem &S, const Rec *R, const float4 *col,
     }
 }
 
-// One block per tile; see the file comment.  Six blocks per SM (40 registers,
-// as many as the shared memory allows) ran 6 % faster than the five that 48
-// registers left room for.
-__global__ void __launch_bounds__(kTB, 6) k_rd_tiles(SplatCfg C, const unsigned *tile_start,
+// One block per tile; see the file comment.  Seven blocks per SM (32
+// registers, 30.2 KB of shared memory with a 576-record window) ran 6 % faster
+// than six (40 registers, 768 records) and eight (448 records) did.
+__global__ void __launch_bounds__(kTB, 7) k_rd_tiles(SplatCfg C, const unsigned *tile_start,
                                                   const unsigned *tile_fill, const Rec *recs, size_t cap,
                                                   const float4 *col, float *buf, unsigned *diag,
                                                   unsigned *est_next) {
