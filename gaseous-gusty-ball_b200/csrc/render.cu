@@ -322,9 +322,9 @@ __device__ __forceinline__ void emit_face(const SplatCfg &C, int f, float px, fl
 // lane finds the particle of its sample by a shuffle search), so particles with
 // many samples do not leave the other lanes idle.  Every sample is drawn on
 // its primary face in lock-step; the other faces with d.c >= 0.5 (near cube
-// edges only) follow.  Five blocks per SM (48 registers, a few bytes
-// spilled) ran 3 % faster than four.
-__global__ void __launch_bounds__(256, 5)
+// edges only) follow.  Six blocks per SM (40 registers, some spilled) ran
+// 4 % faster than five (48 registers) and eight (32).
+__global__ void __launch_bounds__(256, 6)
     k_rd_fill(int n, SplatCfg C, const float *prev, const float *pos, const unsigned *tile_start, unsigned *tile_fill,
               Rec *recs, size_t cap, unsigned *diag) {
     if (tile_start[C.ntiles] > cap) return;  // the host grows the record buffer and runs this again
