@@ -229,6 +229,32 @@ def test_fp32_path_error_vs_fp64_oracle(gpu, orc64):
 
 # ---------------------------------------------------------------- render
 
+@pytest.mark.parametrize("radius", [1.0, 2.5])
+def test_deposit_near_cube_edges_and_corners(gpu, orc32, radius):
+    """Arcs that start within a few texels of the cube's edges and corners,
+    where a sample also lands on neighbouring faces: the record fill projects
+    a sample onto a secondary face only where its footprint can reach that
+    face's texels, which must leave the faces equal to the restatement's."""
+    rng = np.random.default_rng(17)
+    n = 2000
+    R = 64
+    # directions with two (edges) or three (corners) components of equal
+    # magnitude, jittered by up to ~3 texels
+    s = rng.choice([-1.0, 1.0], size=(n, 3))
+    d = s.copy()
+    edge = rng.random(n) < 0.7
+    zero_axis = rng.integers(0, 3, size=n)
+    d[edge, zero_axis[edge]] = rng.uniform(-0.9, 0.9, size=int(edge.sum()))
+    d += (3.0 / R) * rng.normal(size=(n, 3))
+    prev = d / np.linalg.norm(d, axis=1, keepdims=True)
+    pos = prev + (2.0 / R) * rng.normal(size=(n, 3))
+    pos /= np.linalg.norm(pos, axis=1, keepdims=True)
+    col = rng.uniform(0.1, 1, size=(n, 4))
+    a = K.deposit(gpu, R, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32), radius=radius)
+    b = K.deposit(orc32, R, prev.astype(np.float32), pos.astype(np.float32), col.astype(np.float32), radius=radius)
+    assert np.max(np.abs(a["faces"] - b["faces"])) <= 1e-6
+
+
 def test_deposit_golden_exact_order(gpu):
     gold = golden("deposit_R48")
     a = K.deposit(gpu, 48, gold["prev"], gold["pos"], gold["col"], fade_steps=3)
