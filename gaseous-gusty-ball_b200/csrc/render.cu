@@ -794,8 +794,7 @@ __global__ void __launch_bounds__(kTB, 7) k_rd_tiles(SplatCfg C, const unsigned 
     const int tile = blockIdx.x, q = threadIdx.x;
     const int R = C.R, ntx = C.ntx;
     const unsigned s0 = __ldg(tile_start + tile);
-    const int m = (int)min(__ldg(tile_fill + tile), __ldg(tile_start + tile + 1) - s0);
-    if (m == 0 && !C.renorm) return;
+    const unsigned fl = __ldg(tile_fill + tile), s1 = __ldg(tile_start + tile + 1);
     const int f = tile / (ntx * ntx), rem = tile - f * ntx * ntx, ty = rem / ntx, tx = rem - ty * ntx;
     TileGeo G;
     G.x0 = tx * kT;
@@ -805,9 +804,14 @@ __global__ void __launch_bounds__(kTB, 7) k_rd_tiles(SplatCfg C, const unsigned 
     float4 *face = reinterpret_cast<float4 *>(buf) + (size_t)f * R * R;
     const int lx = q % kT, ly = q / kT;
     const bool inside = lx < G.tw && ly < G.th;
+    // the texel is requested together with the tile's record count (before
+    // knowing whether the tile has records), so that the two round trips
+    // overlap; an empty tile then returns with the texel unused
     float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (inside) d = face[(size_t)(G.y0 + ly) * R + G.x0 + lx];
+    const int m = (int)min(fl, s1 - s0);
+    if (m == 0 && !C.renorm) return;
     if (inside) {
-        d = face[(size_t)(G.y0 + ly) * R + G.x0 + lx];
         if (C.renorm) {
             d.x *= C.scale;
             d.y *= C.scale;
