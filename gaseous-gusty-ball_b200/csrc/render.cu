@@ -8,7 +8,9 @@
 // This library reaches the same per-texel order without a global sort:
 //   1. count:  every particle reserves, on each 16x16 texel tile its arc may
 //              touch (FP32 conservative bound), one record slot per sample
-//              (FP32 upper bound on the sample count) — atomics;
+//              (FP32 upper bound on the sample count) — atomics; from the
+//              second deposit on, each tile reserves instead from the largest
+//              count of the previous deposit around it (no counting pass);
 //   2. scan:   tile offsets (one block);
 //   3. fill:   every particle expands its samples exactly (FP64, as upstream)
 //              once and writes one record (order key, px, py) per (sample,
@@ -939,11 +941,11 @@ static void deposit_fill_tiles(Render *r, const Particles *P, RenderPriv *Pv, co
 // The whole deposit without a host round trip: queues the slot reservation,
 // scan, fill and compositing and the copies of the reserved total and the
 // overflow count.  The reservation is exact (k_rd_count) for the first deposit
-// and estimated from the previous deposit's per-tile record counts (neighbourhood maxima) afterwards
-// (no counting pass), except for the b deposits after an estimate overflowed
-// (b doubles with every overflow up to 64 and halves with every estimate that
-// fits).  render_deposit_collect (after a synchronisation of the
-// stream) checks the outcome.  Fill and compositing skip the whole deposit
+// and estimated from the neighbourhood maxima of the previous deposit's
+// per-tile record counts afterwards (no counting pass), except for the b
+// deposits after an estimate overflowed (b doubles with every overflow up to
+// 64 and halves with every estimate that fits).  render_deposit_collect
+// (after a synchronisation of the stream) checks the outcome.  Fill and compositing skip the whole deposit
 // (the face buffer is untouched) when the record buffer was too small, and
 // compositing skips it when an estimated tile overflowed.  The host then grows
 // the buffer and runs them again on the same reservations, or repeats the
