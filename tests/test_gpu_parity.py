@@ -778,6 +778,8 @@ def test_deposit_overflow_backoff(gpu, orc32):
                 got.append(int(api.lib.ggb_render_repeats(C.byref(sp.r))))
         if name == "gpu":
             assert got == expect_repeats, got
+            # of those, one followed a growth of the record buffer (deposit 6)
+            assert int(api.lib.ggb_render_repeats_grown(C.byref(sp.r))) == 1
         out[name] = sp.faces()
         sp.free()
         for ps in sets:
